@@ -1,0 +1,839 @@
+/*
+ * oracle.c -- CPU restatement of the cfdsfemmpi per-time-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity checker for the CUDA
+ * library in cfdsfemmpi_b200/csrc and the timed CPU baseline of bench.py's
+ * reference arm.  Nothing in the product links, loads or calls it.
+ *
+ * What it restates (file:line within the reference project):
+ *   - element routines, active "semi-implicit type B" variants:
+ *       quad4  src/base/LagrangeElem2DNavierStokesQuad4Node.cpp:36-113, 683-970
+ *       tri3   src/base/LagrangeElem2DNavierStokesTria3Node.cpp:36-113, 683-968
+ *       hex8   src/base/LagrangeElem3DNavierStokesHexa8Node.cpp:31-106, 764-1074
+ *       tet4   src/base/LagrangeElem3DNavierStokesTetra4Node.cpp:31-112, 769-1078
+ *   - basis functions  src/base/BasisFunctionsLagrange.cpp:18-186 (mapping),
+ *       517-546 (tria p=1), 703-731 (quad p=1), 889-910 (tetra p=1),
+ *       1035-1079 (hexa p=1, including its derivative table as written)
+ *   - quadrature  src/base/UtilitiesQuadrature.cpp:17-28, 224-257, 263-301, 448-455
+ *   - stabilisation  src/base/stabilisationRoutines.h:128-143 (algo3)
+ *   - per-element Dirichlet lifting  src/base/StabFEM2.cpp:678-703
+ *   - scatter into the free-dof matrix  src/base/SolverPetsc.cpp:304-314
+ *   - free-dof pattern  src/base/StabFEM2.cpp:57-81, 192-227
+ *   - Krylov solve: PETSc 3.10.5 KSPGMRES with classical Gram-Schmidt (no
+ *     refinement), left preconditioning, preconditioned-residual norm,
+ *     x0 = 0, and KSPConvergedDefault; PC "jacobi" (inverse diagonal).  PETSc
+ *     is a third-party dependency that is not part of the reference tree; the
+ *     algorithm below is its published one, called from SolverPetsc.cpp:253.
+ *
+ * Build: oracle/Makefile (gcc -O2 -ffp-contract=off -fopenmp).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_PI 3.141592653589793238462643383279502884197169399375105
+
+enum { ORC_TRI3 = 0, ORC_QUAD4 = 1, ORC_TET4 = 2, ORC_HEX8 = 3 };
+
+static void einfo(int et, int *ndim, int *npe, int *ngp)
+{
+  switch (et) {
+    case ORC_TRI3:  *ndim = 2; *npe = 3; *ngp = 1; break;
+    case ORC_QUAD4: *ndim = 2; *npe = 4; *ngp = 4; break;
+    case ORC_TET4:  *ndim = 3; *npe = 4; *ngp = 1; break;
+    default:        *ndim = 3; *npe = 8; *ngp = 8; break;
+  }
+}
+
+int orc_element_info(int et, int *ndim, int *npe, int *ngp)
+{
+  einfo(et, ndim, npe, ngp);
+  return 0;
+}
+
+/* ---------------- quadrature (UtilitiesQuadrature.cpp) ---------------- */
+static void gauss_points(int et, double gp[][3], double *w)
+{
+  const double g2[2] = {-0.577350269189626, 0.577350269189626};
+  int ind = 0;
+  if (et == ORC_QUAD4) {           /* :224-257, xi1 fastest */
+    for (int jj = 0; jj < 2; jj++)
+      for (int ii = 0; ii < 2; ii++) {
+        gp[ind][0] = g2[ii]; gp[ind][1] = g2[jj]; gp[ind][2] = 0.0;
+        w[ind] = 1.0 * 1.0; ind++;
+      }
+  } else if (et == ORC_TRI3) {     /* tri3 calls getGaussPointsQuad(1): (0,0), w = 2*2 */
+    gp[0][0] = 0.0; gp[0][1] = 0.0; gp[0][2] = 0.0; w[0] = 2.0 * 2.0;
+  } else if (et == ORC_TET4) {     /* :448-455 */
+    gp[0][0] = 0.25; gp[0][1] = 0.25; gp[0][2] = 0.25; w[0] = 1.0 / 6.0;
+  } else {                         /* :263-301, xi1 fastest, then xi2, then xi3 */
+    for (int kk = 0; kk < 2; kk++)
+      for (int jj = 0; jj < 2; jj++)
+        for (int ii = 0; ii < 2; ii++) {
+          gp[ind][0] = g2[ii]; gp[ind][1] = g2[jj]; gp[ind][2] = g2[kk];
+          w[ind] = 1.0 * 1.0 * 1.0; ind++;
+        }
+  }
+}
+
+/* ---------------- reference-element basis (BasisFunctionsLagrange.cpp) -- */
+static void basis_ref(int et, const double *xi, double *N, double *d1, double *d2, double *d3)
+{
+  if (et == ORC_TRI3) {
+    double xi3 = 1.0 - xi[0] - xi[1];
+    N[0] = xi3; N[1] = xi[0]; N[2] = xi[1];
+    d1[0] = -1.0; d1[1] = 1.0; d1[2] = 0.0;
+    d2[0] = -1.0; d2[1] = 0.0; d2[2] = 1.0;
+  } else if (et == ORC_QUAD4) {
+    double b1 = 0.5 * (1.0 - xi[1]), b2 = 0.5 * (1.0 + xi[1]);
+    double db1 = -0.5, db2 = 0.5;
+    double a1 = 0.5 * (1.0 - xi[0]), a2 = 0.5 * (1.0 + xi[0]);
+    double da1 = -0.5, da2 = 0.5;
+    N[0] = b1 * a1; N[1] = b1 * a2; N[2] = b2 * a2; N[3] = b2 * a1;
+    d1[0] = b1 * da1; d1[1] = b1 * da2; d1[2] = b2 * da2; d1[3] = b2 * da1;
+    d2[0] = db1 * a1; d2[1] = db1 * a2; d2[2] = db2 * a2; d2[3] = db2 * a1;
+  } else if (et == ORC_TET4) {
+    double xi4 = 1.0 - xi[0] - xi[1] - xi[2];
+    N[0] = xi4; N[1] = xi[0]; N[2] = xi[1]; N[3] = xi[2];
+    d1[0] = -1.0; d1[1] = 1.0; d1[2] = 0.0; d1[3] = 0.0;
+    d2[0] = -1.0; d2[1] = 0.0; d2[2] = 1.0; d2[3] = 0.0;
+    d3[0] = -1.0; d3[1] = 0.0; d3[2] = 0.0; d3[3] = 1.0;
+  } else {
+    /* BasisFunctionsLagrange.cpp:1037-1078.  The xi2 and xi3 derivative
+     * rows pair local nodes 2<->3 and 6<->7 differently from N; this is the
+     * reference's table and is kept as written. */
+    double v11 = 1.0 - xi[0], v12 = 1.0 + xi[0];
+    double v21 = 1.0 - xi[1], v22 = 1.0 + xi[1];
+    double v31 = 1.0 - xi[2], v32 = 1.0 + xi[2];
+    N[0] = 0.125 * v11 * v21 * v31; N[1] = 0.125 * v12 * v21 * v31;
+    N[2] = 0.125 * v12 * v22 * v31; N[3] = 0.125 * v11 * v22 * v31;
+    N[4] = 0.125 * v11 * v21 * v32; N[5] = 0.125 * v12 * v21 * v32;
+    N[6] = 0.125 * v12 * v22 * v32; N[7] = 0.125 * v11 * v22 * v32;
+    d1[0] = -0.125 * v21 * v31; d1[1] = 0.125 * v21 * v31;
+    d1[2] = 0.125 * v22 * v31;  d1[3] = -0.125 * v22 * v31;
+    d1[4] = -0.125 * v21 * v32; d1[5] = 0.125 * v21 * v32;
+    d1[6] = 0.125 * v22 * v32;  d1[7] = -0.125 * v22 * v32;
+    d2[0] = -0.125 * v11 * v31; d2[1] = -0.125 * v12 * v31;
+    d2[2] = 0.125 * v11 * v31;  d2[3] = 0.125 * v12 * v31;
+    d2[4] = -0.125 * v11 * v32; d2[5] = -0.125 * v12 * v32;
+    d2[6] = 0.125 * v11 * v32;  d2[7] = 0.125 * v12 * v32;
+    d3[0] = -0.125 * v11 * v21; d3[1] = -0.125 * v12 * v21;
+    d3[2] = -0.125 * v11 * v22; d3[3] = -0.125 * v12 * v22;
+    d3[4] = 0.125 * v11 * v21;  d3[5] = 0.125 * v12 * v21;
+    d3[6] = 0.125 * v11 * v22;  d3[7] = 0.125 * v12 * v22;
+  }
+}
+
+/* Physical-space basis at one quadrature point: BasisFunctionsLagrange.cpp:18-97
+ * (2D, closed-form inverse) and :101-186 (3D, determinant and inverse of the
+ * 3x3 mapping gradient B(a,b) = d x_b / d xi_a, written here by cofactors). */
+static void basis_phys(int et, int ndim, int npe, const double *xi, const double *X,
+                       double *N, double *dx, double *dy, double *dz, double *Jac)
+{
+  double d1[8], d2[8], d3[8];
+  basis_ref(et, xi, N, d1, d2, d3);
+  if (ndim == 2) {
+    double B00 = 0, B01 = 0, B10 = 0, B11 = 0;
+    for (int ii = 0; ii < npe; ii++) {
+      double xx = X[ii * 2 + 0], yy = X[ii * 2 + 1];
+      B00 += (xx * d1[ii]); B10 += (xx * d2[ii]);
+      B01 += (yy * d1[ii]); B11 += (yy * d2[ii]);
+    }
+    double J = B00 * B11 - B01 * B10;
+    double detinv = 1.0 / J;
+    double I00 = B11 * detinv, I01 = -B01 * detinv, I10 = -B10 * detinv, I11 = B00 * detinv;
+    for (int ii = 0; ii < npe; ii++) {
+      dx[ii] = d1[ii] * I00 + d2[ii] * I01;
+      dy[ii] = d1[ii] * I10 + d2[ii] * I11;
+    }
+    *Jac = J;
+  } else {
+    double B[3][3] = {{0}};
+    for (int ii = 0; ii < npe; ii++) {
+      double xx = X[ii * 3 + 0], yy = X[ii * 3 + 1], zz = X[ii * 3 + 2];
+      B[0][0] += (xx * d1[ii]); B[1][0] += (xx * d2[ii]); B[2][0] += (xx * d3[ii]);
+      B[0][1] += (yy * d1[ii]); B[1][1] += (yy * d2[ii]); B[2][1] += (yy * d3[ii]);
+      B[0][2] += (zz * d1[ii]); B[1][2] += (zz * d2[ii]); B[2][2] += (zz * d3[ii]);
+    }
+    /* cofactors C(i,j); inverse(i,j) = C(j,i)/det */
+    double C[3][3];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+        C[i][j] = B[i1][j1] * B[i2][j2] - B[i1][j2] * B[i2][j1];
+      }
+    double J = B[0][0] * C[0][0] + B[0][1] * C[0][1] + B[0][2] * C[0][2];
+    double invdet = 1.0 / J;
+    double I[3][3];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) I[i][j] = C[j][i] * invdet;
+    for (int ii = 0; ii < npe; ii++) {
+      dx[ii] = d1[ii] * I[0][0] + d2[ii] * I[0][1] + d3[ii] * I[0][2];
+      dy[ii] = d1[ii] * I[1][0] + d2[ii] * I[1][1] + d3[ii] * I[1][2];
+      dz[ii] = d1[ii] * I[2][0] + d2[ii] * I[2][1] + d3[ii] * I[2][2];
+    }
+    *Jac = J;
+  }
+}
+
+/*
+ * One element: K (nsize x nsize, row-major, local index node*ndof+dof) and F.
+ * X: npe*ndim coordinates; prev/cur/dotcur: npe*ndof nodal values of
+ * solnPrev, solnCur, solnDotCur.  elemData as StabFEM::readControlParameters
+ * fills it (StabFEM.cpp:285-294): [0]=rho, [1]=mu, [8..10]=SUPG/PSPG/LSIC.
+ * td: SolutionData::td (UtilitiesGeneral.cpp:5-205).
+ * info (optional, 2 doubles): elemVol, charlen.
+ * Returns 0, or -1 for a negative Jacobian (the reference exits there).
+ */
+int orc_element(int et, const double *X, const double *prev, const double *cur,
+                const double *dotcur, const double *elemData, const double *td,
+                double *K, double *F, double *info)
+{
+  int ndim, npe, ngp;
+  einfo(et, &ndim, &npe, &ngp);
+  const int ndof = ndim + 1, nsize = npe * ndof;
+  double gpx[8][3], gw[8];
+  gauss_points(et, gpx, gw);
+
+  /* prepareElemData */
+  double Nv[8][8], Dx[8][8], Dy[8][8], Dz[8][8], dv[8];
+  double elemVol = 0.0;
+  int neg = 0;
+  for (int gp = 0; gp < ngp; gp++) {
+    double Jac;
+    basis_phys(et, ndim, npe, gpx[gp], X, Nv[gp], Dx[gp], Dy[gp], Dz[gp], &Jac);
+    if (Jac < 0.0) neg = 1;
+    dv[gp] = gw[gp] * Jac;
+    elemVol += dv[gp];
+  }
+  double charlen = (ndim == 2) ? sqrt(4.0 * fabs(elemVol) / ORC_PI)
+                               : pow(6.0 * fabs(elemVol) / ORC_PI, 1.0 / 3.0);
+  if (info) { info[0] = elemVol; info[1] = charlen; }
+
+  /* calcStiffnessAndResidual (active semi-implicit type B routine) */
+  const double CI = (ndim == 2) ? 4.0 : 10.0;
+  const double cs = (et == ORC_HEX8) ? -1.0 : 1.0;   /* hex8 continuity row sign */
+  const int supg = (ndim == 2);                       /* SUPG is commented out in 3D */
+  double fact = 4.0 / charlen / charlen;
+  double G[3] = {fact, fact, (ndim == 3) ? fact : 0.0};
+  double sumG2 = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+  double trG = G[0] + G[1] + G[2];
+
+  const double rho = elemData[0], mu = elemData[1];
+  const double af = td[2], acceFact = td[8];
+  const double muTaf = mu * af;
+
+  memset(K, 0, sizeof(double) * nsize * nsize);
+  memset(F, 0, sizeof(double) * nsize);
+
+  for (int gp = 0; gp < ngp; gp++) {
+    const double *N = Nv[gp];
+    const double *dN[3] = {Dx[gp], Dy[gp], Dz[gp]};
+    double velPrev[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, velDot[3] = {0, 0, 0}, dp[3] = {0, 0, 0};
+    double gradPrev[3][3] = {{0}}, grad[3][3] = {{0}};
+    double pres = 0.0;
+    for (int ii = 0; ii < npe; ii++) {
+      const int TI = ii * ndof;
+      for (int a = 0; a < ndim; a++) {
+        double b = prev[TI + a];
+        velPrev[a] += b * N[ii];
+        for (int c = 0; c < ndim; c++) gradPrev[a][c] += b * dN[c][ii];
+      }
+      for (int a = 0; a < ndim; a++) {
+        double b = cur[TI + a];
+        vel[a] += b * N[ii];
+        for (int c = 0; c < ndim; c++) grad[a][c] += b * dN[c][ii];
+      }
+      double b4 = cur[TI + ndim];
+      pres += b4 * N[ii];
+      for (int c = 0; c < ndim; c++) dp[c] += b4 * dN[c][ii];
+      for (int a = 0; a < ndim; a++) velDot[a] += dotcur[TI + a] * N[ii];
+    }
+    double stress[3][3];
+    for (int a = 0; a < ndim; a++)
+      for (int c = 0; c < ndim; c++) stress[a][c] = mu * grad[a][c];
+    for (int a = 0; a < ndim; a++) stress[a][a] -= pres;
+
+    double gradTvel[3], res2[3], rStab[3];
+    for (int a = 0; a < ndim; a++) {
+      double t1 = 0, t2 = 0, t3 = 0;
+      for (int c = 0; c < ndim; c++) {
+        t1 += gradPrev[a][c] * vel[c];
+        t2 += grad[a][c] * velPrev[c];
+        t3 += gradPrev[a][c] * velPrev[c];
+      }
+      gradTvel[a] = t1 + t2 - t3;
+    }
+    for (int a = 0; a < ndim; a++) {
+      res2[a] = rho * (velDot[a] + gradTvel[a] - 0.0);
+      rStab[a] = res2[a] - mu * 0.0 + dp[a];
+    }
+
+    /* evaluateStabParams_algo3 at velPrev (3-vector, zero 3rd entry in 2D) */
+    double uGu = 0.0;
+    for (int a = 0; a < 3; a++) {
+      double ua = (a < ndim) ? velPrev[a] : 0.0;
+      uGu += ua * (G[a] * ua);
+    }
+    double tau0 = uGu + CI * (mu * mu / rho / rho) * sumG2;
+    tau0 = 1.0 / sqrt(tau0);
+    double tau2 = 1.0 / (tau0 * trG);
+    tau0 = tau0 / rho;
+    double tau1 = tau0;
+    tau0 *= elemData[8];
+    tau1 *= elemData[9];
+    tau2 *= elemData[10];
+    (void)tau2;                                   /* LSIC terms are commented out */
+
+    const double dvol = dv[gp];
+    for (int ii = 0; ii < npe; ii++) {
+      const int TI = ndof * ii;
+      double bb[3], b4, bm[3], b8;
+      for (int a = 0; a < ndim; a++) bb[a] = dN[a][ii] * dvol;
+      b4 = N[ii] * dvol;
+      for (int a = 0; a < ndim; a++) bm[a] = muTaf * bb[a];
+      b8 = af * b4;
+      double Da = 0.0;
+      for (int a = 0; a < ndim; a++) Da += velPrev[a] * bb[a];
+      Da = rho * Da * tau0;
+
+      for (int jj = 0; jj < npe; jj++) {
+        const int TJ = ndof * jj;
+        double fact2 = rho * acceFact * N[jj];
+        double f = b4 * fact2;
+        double dif = 0.0;
+        for (int a = 0; a < ndim; a++) dif += bm[a] * dN[a][jj];
+        f += dif;
+        for (int a = 0; a < ndim; a++) K[(TI + a) * nsize + TJ + a] += f;
+
+        double gradN[3][3];
+        double rN = rho * N[jj];
+        for (int a = 0; a < ndim; a++)
+          for (int c = 0; c < ndim; c++) gradN[a][c] = gradPrev[a][c] * rN;
+        double Db = 0.0;
+        for (int a = 0; a < ndim; a++) Db += velPrev[a] * dN[a][jj];
+        Db = rho * Db;
+        for (int a = 0; a < ndim; a++) gradN[a][a] += Db;
+
+        for (int a = 0; a < ndim; a++)
+          for (int c = 0; c < ndim; c++) K[(TI + a) * nsize + TJ + c] += (b8 * gradN[a][c]);
+        for (int a = 0; a < ndim; a++) K[(TI + a) * nsize + TJ + ndim] -= (bb[a] * af * N[jj]);
+        for (int c = 0; c < ndim; c++) K[(TI + ndim) * nsize + TJ + c] += cs * (b8 * dN[c][jj]);
+
+        for (int a = 0; a < ndim; a++)
+          for (int c = 0; c < ndim; c++) gradN[a][c] *= af;
+        double Dj[3][4];
+        for (int a = 0; a < ndim; a++) {
+          for (int c = 0; c < ndim; c++) Dj[a][c] = gradN[a][c] + ((a == c) ? fact2 : 0.0);
+          Dj[a][ndim] = af * dN[a][jj];
+        }
+        if (supg) {
+          for (int a = 0; a < ndim; a++)
+            for (int c = 0; c <= ndim; c++) K[(TI + a) * nsize + TJ + c] += Da * Dj[a][c];
+        }
+        for (int c = 0; c <= ndim; c++) {
+          double s = 0.0;
+          for (int a = 0; a < ndim; a++) s += bb[a] * Dj[a][c];
+          K[(TI + ndim) * nsize + TJ + c] += cs * (s * tau1);
+        }
+      }
+
+      for (int a = 0; a < ndim; a++) {
+        double s = b4 * res2[a];
+        for (int c = 0; c < ndim; c++) s += bb[c] * stress[a][c];
+        F[TI + a] -= s;
+      }
+      double tr = 0.0;
+      for (int a = 0; a < ndim; a++) tr += grad[a][a];
+      F[TI + ndim] -= cs * (b4 * tr);
+      if (supg)
+        for (int a = 0; a < ndim; a++) F[TI + a] -= Da * rStab[a];
+      double s = 0.0;
+      for (int a = 0; a < ndim; a++) s += bb[a] * rStab[a];
+      F[TI + ndim] -= cs * (tau1 * s);
+    }
+  }
+  return neg ? -1 : 0;
+}
+
+/* ---------------- free-dof pattern (StabFEM2.cpp:57-81, 192-227) -------- */
+
+/* node -> sorted unique neighbour nodes (nodes sharing an element) */
+static int build_node_graph(int nNode, int nElem, int npe, const int *conn, int **nptr_out, int **nadj_out)
+{
+  int *ecount = calloc(nNode + 1, sizeof(int));
+  for (int e = 0; e < nElem; e++)
+    for (int a = 0; a < npe; a++) ecount[conn[e * npe + a] + 1]++;
+  for (int n = 0; n < nNode; n++) ecount[n + 1] += ecount[n];
+  int *elist = malloc(sizeof(int) * (size_t)ecount[nNode]);
+  int *fill = calloc(nNode, sizeof(int));
+  for (int e = 0; e < nElem; e++)
+    for (int a = 0; a < npe; a++) {
+      int n = conn[e * npe + a];
+      elist[ecount[n] + fill[n]++] = e;
+    }
+  int *nptr = calloc(nNode + 1, sizeof(int));
+  int *mark = malloc(sizeof(int) * nNode);
+  for (int n = 0; n < nNode; n++) mark[n] = -1;
+  /* count */
+  for (int n = 0; n < nNode; n++) {
+    int cnt = 0;
+    for (int k = ecount[n]; k < ecount[n + 1]; k++) {
+      int e = elist[k];
+      for (int a = 0; a < npe; a++) {
+        int m = conn[e * npe + a];
+        if (mark[m] != n) { mark[m] = n; cnt++; }
+      }
+    }
+    nptr[n + 1] = nptr[n] + cnt;
+  }
+  int *nadj = malloc(sizeof(int) * (size_t)nptr[nNode]);
+  for (int n = 0; n < nNode; n++) mark[n] = -1;
+  for (int n = 0; n < nNode; n++) {
+    int pos = nptr[n];
+    for (int k = ecount[n]; k < ecount[n + 1]; k++) {
+      int e = elist[k];
+      for (int a = 0; a < npe; a++) {
+        int m = conn[e * npe + a];
+        if (mark[m] != n) { mark[m] = n; nadj[pos++] = m; }
+      }
+    }
+    /* insertion sort (short lists) */
+    for (int i = nptr[n] + 1; i < nptr[n + 1]; i++) {
+      int v = nadj[i], j = i - 1;
+      while (j >= nptr[n] && nadj[j] > v) { nadj[j + 1] = nadj[j]; j--; }
+      nadj[j + 1] = v;
+    }
+  }
+  free(ecount); free(elist); free(fill); free(mark);
+  *nptr_out = nptr; *nadj_out = nadj;
+  return 0;
+}
+
+/* dofmap[n*ndof+d] = free index or -1.  Pass colidx == NULL to only count:
+ * returns nnz.  rowptr has ntot+1 entries. */
+long orc_pattern(int nNode, int ndof, int nElem, int npe, const int *conn, const int *dofmap,
+                 int ntot, int *rowptr, int *colidx)
+{
+  int *nptr, *nadj;
+  build_node_graph(nNode, nElem, npe, conn, &nptr, &nadj);
+  long nnz = 0;
+  for (int n = 0; n < nNode; n++) {
+    for (int d = 0; d < ndof; d++) {
+      int r = dofmap[n * ndof + d];
+      if (r < 0) continue;
+      rowptr[r] = (int)nnz;
+      for (int k = nptr[n]; k < nptr[n + 1]; k++) {
+        int m = nadj[k];
+        for (int e2 = 0; e2 < ndof; e2++) {
+          int c = dofmap[m * ndof + e2];
+          if (c < 0) continue;
+          if (colidx) colidx[nnz] = c;
+          nnz++;
+        }
+      }
+    }
+  }
+  rowptr[ntot] = (int)nnz;
+  free(nptr); free(nadj);
+  return nnz;
+}
+
+/* ---------------- assembly into the free-dof CSR ---------------- */
+static inline int find_col(const int *colidx, int lo, int hi, int c)
+{
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (colidx[mid] < c) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+static int assemble_one(int et, int e, int ndim, int npe, const int *conn, const double *coords,
+                        const int *dofmap, const double *solnPrev, const double *solnCur,
+                        const double *solnDotCur, const double *solnApplied,
+                        const double *elemData, const double *td, int iter, int want_K,
+                        const int *rowptr, const int *colidx, double *vals, double *rhs)
+{
+  const int ndof = ndim + 1, nsize = npe * ndof;
+  double X[24], pv[32], cv[32], dc[32], K[32 * 32], F[32];
+  int fa[32], gdof[32];
+  for (int a = 0; a < npe; a++) {
+    int n = conn[e * npe + a];
+    for (int c = 0; c < ndim; c++) X[a * ndim + c] = coords[(size_t)n * ndim + c];
+    for (int d = 0; d < ndof; d++) {
+      size_t g = (size_t)n * ndof + d;
+      pv[a * ndof + d] = solnPrev[g];
+      cv[a * ndof + d] = solnCur[g];
+      dc[a * ndof + d] = solnDotCur[g];
+      fa[a * ndof + d] = dofmap[g];
+      gdof[a * ndof + d] = (int)g;
+    }
+  }
+  int rc = orc_element(et, X, pv, cv, dc, elemData, td, K, F, NULL);
+  if (iter == 0) {                                  /* StabFEM2.cpp:678-703 */
+    for (int ii = 0; ii < nsize; ii++) {
+      if (fa[ii] == -1) {
+        double fact = solnApplied[gdof[ii]];
+        if (fabs(fact) > 1.0e-10) {
+          for (int jj = 0; jj < nsize; jj++)
+            if (fa[jj] != -1) F[jj] -= K[jj * nsize + ii] * fact;
+        }
+      }
+    }
+  }
+  for (int ii = 0; ii < nsize; ii++) {              /* SolverPetsc.cpp:304-314 */
+    int r = fa[ii];
+    if (r < 0) continue;
+    rhs[r] += F[ii];
+    if (!want_K) continue;
+    int lo = rowptr[r], hi = rowptr[r + 1];
+    for (int jj = 0; jj < nsize; jj++) {
+      int c = fa[jj];
+      if (c < 0) continue;
+      int p = find_col(colidx, lo, hi, c);
+      vals[p] += K[ii * nsize + jj];
+    }
+  }
+  return rc;
+}
+
+/*
+ * Assemble all elements for one Newton iteration (StabFEM2.cpp:669-708).
+ * vals/rhs are zeroed here (SolverPetsc::zeroMtx).  With ncolors == 0 the
+ * elements run serially in element order (the reference's order); with a
+ * colouring (color_ptr/color_elems) they run colour by colour, in parallel
+ * inside a colour, so every entry receives its sums in a fixed order.
+ * want_K == 0 assembles only the residual.  Returns the number of elements
+ * with a negative Jacobian.
+ */
+int orc_assemble(int et, int nNode, int nElem, const int *conn, const double *coords,
+                 const int *dofmap, const double *solnPrev, const double *solnCur,
+                 const double *solnDotCur, const double *solnApplied, const double *elemData,
+                 const double *td, int iter, int want_K, const int *rowptr, const int *colidx,
+                 long nnz, double *vals, int ntot, double *rhs, int ncolors,
+                 const int *color_ptr, const int *color_elems, int nthreads)
+{
+  int ndim, npe, ngp;
+  einfo(et, &ndim, &npe, &ngp);
+  (void)nNode;
+  if (want_K) memset(vals, 0, sizeof(double) * (size_t)nnz);
+  memset(rhs, 0, sizeof(double) * (size_t)ntot);
+  int nneg = 0;
+  if (ncolors <= 0) {
+    for (int e = 0; e < nElem; e++)
+      nneg += assemble_one(et, e, ndim, npe, conn, coords, dofmap, solnPrev, solnCur, solnDotCur,
+                           solnApplied, elemData, td, iter, want_K, rowptr, colidx, vals, rhs) != 0;
+  } else {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    for (int c = 0; c < ncolors; c++) {
+      int lo = color_ptr[c], hi = color_ptr[c + 1];
+      int neg_c = 0;
+#pragma omp parallel for schedule(static) reduction(+ : neg_c)
+      for (int k = lo; k < hi; k++)
+        neg_c += assemble_one(et, color_elems[k], ndim, npe, conn, coords, dofmap, solnPrev, solnCur,
+                              solnDotCur, solnApplied, elemData, td, iter, want_K, rowptr, colidx,
+                              vals, rhs) != 0;
+      nneg += neg_c;
+    }
+  }
+  return nneg;
+}
+
+/* ---------------- vector kernels ---------------- */
+static double vdot(int n, const double *a, const double *b)
+{
+  double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : s)
+  for (int i = 0; i < n; i++) s += a[i] * b[i];
+  return s;
+}
+
+double orc_norm2(int n, const double *a) { return sqrt(vdot(n, a, a)); }
+
+static void spmv(int n, const int *rowptr, const int *colidx, const double *vals, const double *x, double *y)
+{
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < n; r++) {
+    double s = 0.0;
+    for (int k = rowptr[r]; k < rowptr[r + 1]; k++) s += vals[k] * x[colidx[k]];
+    y[r] = s;
+  }
+}
+
+void orc_spmv(int n, const int *rowptr, const int *colidx, const double *vals, const double *x, double *y, int nthreads)
+{
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  spmv(n, rowptr, colidx, vals, x, y);
+}
+
+/* Point-block Jacobi blocks for pc == 2: runs of consecutive free dofs that
+ * belong to one node (the free numbering is node-major, so a node's free
+ * dofs are contiguous).  Set by orc_set_blocks before orc_gmres. */
+static int g_nblk = 0;
+static const int *g_blk_ptr = NULL;
+
+void orc_set_blocks(int nblk, const int *blk_ptr) { g_nblk = nblk; g_blk_ptr = blk_ptr; }
+
+/* invert a small dense row-major block in place (Gauss-Jordan, partial pivoting) */
+static int small_inverse(int b, double *A)
+{
+  double inv[16];
+  for (int i = 0; i < b * b; i++) inv[i] = 0.0;
+  for (int i = 0; i < b; i++) inv[i * b + i] = 1.0;
+  for (int c = 0; c < b; c++) {
+    int piv = c;
+    for (int r = c + 1; r < b; r++) if (fabs(A[r * b + c]) > fabs(A[piv * b + c])) piv = r;
+    if (A[piv * b + c] == 0.0) return -1;
+    if (piv != c)
+      for (int k = 0; k < b; k++) {
+        double t = A[c * b + k]; A[c * b + k] = A[piv * b + k]; A[piv * b + k] = t;
+        t = inv[c * b + k]; inv[c * b + k] = inv[piv * b + k]; inv[piv * b + k] = t;
+      }
+    double d = 1.0 / A[c * b + c];
+    for (int k = 0; k < b; k++) { A[c * b + k] *= d; inv[c * b + k] *= d; }
+    for (int r = 0; r < b; r++) {
+      if (r == c) continue;
+      double f = A[r * b + c];
+      if (f == 0.0) continue;
+      for (int k = 0; k < b; k++) { A[r * b + k] -= f * A[c * b + k]; inv[r * b + k] -= f * inv[c * b + k]; }
+    }
+  }
+  for (int i = 0; i < b * b; i++) A[i] = inv[i];
+  return 0;
+}
+
+/* PETSc KSPConvergedReason values used here */
+#define R_ITERATING 0
+#define R_RTOL 2
+#define R_ATOL 3
+#define R_DIV_NULL (-2)
+#define R_DIV_ITS (-3)
+#define R_DIV_DTOL (-4)
+#define R_DIV_BREAKDOWN (-5)
+#define R_DIV_NANORINF (-9)
+
+static void pc_apply(int n, int pc, const double *dinv, const double *binv, const double *r, double *z)
+{
+  if (pc != 2) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) z[i] = dinv[i] * r[i];
+    return;
+  }
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g_nblk; k++) {
+    int r0 = g_blk_ptr[k], bs = g_blk_ptr[k + 1] - r0;
+    const double *B = binv + (size_t)k * 16;
+    for (int i = 0; i < bs; i++) {
+      double s = 0.0;
+      for (int j = 0; j < bs; j++) s += B[i * bs + j] * r[r0 + j];
+      z[r0 + i] = s;
+    }
+  }
+}
+
+typedef struct {
+  double rnorm0, ttol;
+  double rtol, atol, dtol;
+} conv_ctx;
+
+static int converged(conv_ctx *c, int n_its, double rnorm)
+{
+  if (n_its == 0) { c->rnorm0 = rnorm; c->ttol = fmax(c->rtol * rnorm, c->atol); }
+  if (rnorm != rnorm || isinf(rnorm)) return R_DIV_NANORINF;
+  if (rnorm <= c->ttol) return (rnorm < c->atol) ? R_ATOL : R_RTOL;
+  if (rnorm >= c->dtol * c->rnorm0) return R_DIV_DTOL;
+  return R_ITERATING;
+}
+
+/*
+ * GMRES(restart) with left preconditioning (pc: 0 none, 1 jacobi, 2 point-block
+ * jacobi over the blocks set by orc_set_blocks), x0 = 0.
+ * Follows PETSc 3.10 KSPSolve_GMRES / KSPGMRESCycle /
+ * KSPGMRESClassicalGramSchmidtOrthogonalization / KSPGMRESUpdateHessenberg /
+ * KSPGMRESBuildSoln.  Returns the KSPConvergedReason; *its_out the iteration
+ * count, *rnorm_out the last preconditioned residual norm.
+ */
+int orc_gmres(int n, const int *rowptr, const int *colidx, const double *vals, int pc,
+              const double *b, double *x, int restart, double rtol, double atol, double dtol,
+              int maxit, int *its_out, double *rnorm_out, int nthreads)
+{
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  const int m = restart;
+  const double haptol = 1.0e-30;
+  double *dinv = malloc(sizeof(double) * n);
+  for (int r = 0; r < n; r++) {
+    double d = 0.0;
+    for (int k = rowptr[r]; k < rowptr[r + 1]; k++)
+      if (colidx[k] == r) d = vals[k];
+    dinv[r] = (pc == 1) ? ((d != 0.0) ? 1.0 / d : 1.0) : 1.0;
+  }
+  double *binv = NULL;
+  if (pc == 2) {
+    binv = calloc((size_t)g_nblk * 16, sizeof(double));
+    for (int k = 0; k < g_nblk; k++) {
+      int r0 = g_blk_ptr[k], bs = g_blk_ptr[k + 1] - r0;
+      double *B = binv + (size_t)k * 16;
+      for (int i = 0; i < bs; i++)
+        for (int p = rowptr[r0 + i]; p < rowptr[r0 + i + 1]; p++) {
+          int c = colidx[p];
+          if (c >= r0 && c < r0 + bs) B[i * bs + (c - r0)] = vals[p];
+        }
+      small_inverse(bs, B);
+    }
+  }
+  double *V = malloc(sizeof(double) * (size_t)n * (m + 1));
+  double *tmp = malloc(sizeof(double) * n);
+  double *H = calloc((size_t)(m + 1) * m, sizeof(double));   /* H[row*m + col] */
+  double *cc = calloc(m, sizeof(double)), *ss = calloc(m, sizeof(double));
+  double *grs = calloc(m + 1, sizeof(double)), *nrs = calloc(m, sizeof(double));
+  double *hh = calloc(m + 1, sizeof(double));
+  conv_ctx cv = {0, 0, rtol, atol, dtol};
+  memset(x, 0, sizeof(double) * n);
+  int its = 0, reason = R_ITERATING, first = 1;
+  double res = 0.0;
+
+  while (reason == R_ITERATING) {
+    /* KSPInitialResidual: r = b - A x (b when x0 = 0), then v0 = M^-1 r */
+    if (first) {
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < n; i++) tmp[i] = b[i];
+    } else {
+      spmv(n, rowptr, colidx, vals, x, tmp);
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < n; i++) tmp[i] = b[i] - tmp[i];
+    }
+    pc_apply(n, pc, dinv, binv, tmp, V);
+    first = 0;
+    /* KSPGMRESCycle */
+    res = sqrt(vdot(n, V, V));
+    if (res != 0.0) {
+      double sc = 1.0 / res;
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < n; i++) V[i] *= sc;
+    }
+    grs[0] = res;
+    int it = 0;
+    if (res == 0.0) { if (its == 0) { cv.rnorm0 = 0; } reason = R_ATOL; break; }
+    reason = converged(&cv, its, res);
+    while (reason == R_ITERATING && it < m && its < maxit) {
+      double *vi = V + (size_t)n * it, *w = V + (size_t)n * (it + 1);
+      spmv(n, rowptr, colidx, vals, vi, tmp);
+      pc_apply(n, pc, dinv, binv, tmp, w);
+      /* classical Gram-Schmidt */
+      for (int j = 0; j <= it; j++) hh[j] = vdot(n, w, V + (size_t)n * j);
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < n; i++) {
+        double s = w[i];
+        for (int j = 0; j <= it; j++) s += (-hh[j]) * V[(size_t)n * j + i];
+        w[i] = s;
+      }
+      for (int j = 0; j <= it; j++) H[j * m + it] = hh[j];
+      double tt = sqrt(vdot(n, w, w));
+      if (tt != 0.0) {
+        double sc = 1.0 / tt;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) w[i] *= sc;
+      }
+      H[(it + 1) * m + it] = tt;
+      double hapbnd = fabs(tt / grs[it]);
+      if (hapbnd > haptol) hapbnd = haptol;
+      int hapend = (tt < hapbnd);
+      /* KSPGMRESUpdateHessenberg */
+      for (int j = 1; j <= it; j++) {
+        double t = H[(j - 1) * m + it];
+        H[(j - 1) * m + it] = cc[j - 1] * t + ss[j - 1] * H[j * m + it];
+        H[j * m + it] = cc[j - 1] * H[j * m + it] - ss[j - 1] * t;
+      }
+      if (!hapend) {
+        double a = H[it * m + it], bq = H[(it + 1) * m + it];
+        double t = sqrt(a * a + bq * bq);
+        if (t == 0.0) { reason = R_DIV_NULL; break; }
+        cc[it] = a / t;
+        ss[it] = bq / t;
+        grs[it + 1] = -(ss[it] * grs[it]);
+        grs[it] = cc[it] * grs[it];
+        H[it * m + it] = cc[it] * a + ss[it] * bq;
+        res = fabs(grs[it + 1]);
+      } else {
+        res = 0.0;
+      }
+      it++;
+      its++;
+      reason = converged(&cv, its, res);
+      if (hapend && reason == R_ITERATING) { reason = R_DIV_BREAKDOWN; break; }
+    }
+    /* KSPGMRESBuildSoln with it-1 */
+    int last = it - 1;
+    if (last >= 0) {
+      if (H[last * m + last] != 0.0) nrs[last] = grs[last] / H[last * m + last];
+      else nrs[last] = 0.0;
+      for (int ii = 1; ii <= last; ii++) {
+        int k = last - ii;
+        double t = grs[k];
+        for (int j = k + 1; j <= last; j++) t = t - H[k * m + j] * nrs[j];
+        nrs[k] = (H[k * m + k] != 0.0) ? t / H[k * m + k] : 0.0;
+      }
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < n; i++) {
+        double s = 0.0;
+        for (int j = 0; j <= last; j++) s += nrs[j] * V[(size_t)n * j + i];
+        x[i] += s;
+      }
+    }
+    if (reason != R_ITERATING) break;
+    if (its >= maxit) { reason = R_DIV_ITS; break; }
+  }
+  if (its_out) *its_out = its;
+  if (rnorm_out) *rnorm_out = res;
+  free(dinv); free(binv); free(V); free(tmp); free(H); free(cc); free(ss); free(grs); free(nrs); free(hh);
+  return reason;
+}
+
+/* greedy element colouring: elements that share a node get different
+ * colours; elements are visited in id order and take the smallest free
+ * colour.  Same rule as the CUDA library's host-side builder. */
+int orc_color(int nNode, int nElem, int npe, const int *conn, int *color)
+{
+  /* node -> elements */
+  int *ecount = calloc(nNode + 1, sizeof(int));
+  for (int e = 0; e < nElem; e++)
+    for (int a = 0; a < npe; a++) ecount[conn[e * npe + a] + 1]++;
+  for (int n = 0; n < nNode; n++) ecount[n + 1] += ecount[n];
+  int *elist = malloc(sizeof(int) * (size_t)ecount[nNode]);
+  int *fill = calloc(nNode, sizeof(int));
+  for (int e = 0; e < nElem; e++)
+    for (int a = 0; a < npe; a++) {
+      int n = conn[e * npe + a];
+      elist[ecount[n] + fill[n]++] = e;
+    }
+  for (int e = 0; e < nElem; e++) color[e] = -1;
+  int ncolors = 0;
+  uint64_t used;
+  for (int e = 0; e < nElem; e++) {
+    used = 0;
+    for (int a = 0; a < npe; a++) {
+      int n = conn[e * npe + a];
+      for (int k = ecount[n]; k < ecount[n + 1]; k++) {
+        int c = color[elist[k]];
+        if (c >= 0 && c < 64) used |= (1ULL << c);
+      }
+    }
+    int c = 0;
+    while (c < 64 && (used & (1ULL << c))) c++;
+    color[e] = c;
+    if (c + 1 > ncolors) ncolors = c + 1;
+  }
+  free(ecount); free(elist); free(fill);
+  return ncolors;
+}
