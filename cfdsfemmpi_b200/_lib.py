@@ -1,0 +1,284 @@
+"""ctypes binding of the C ABI in include/cfdgpu.h (libcfdgpu.so, in-tree).
+
+There is no CPU fallback: if the library is missing or cannot be loaded the
+import of the GPU path raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcfdgpu.so")
+
+# the symbols declared in include/cfdgpu.h, in declaration order
+EXPORTS = [
+    "cfdgpu_create", "cfdgpu_destroy", "cfdgpu_last_error", "cfdgpu_step", "cfdgpu_get_solution",
+    "cfdgpu_set_solution", "cfdgpu_device_solution", "cfdgpu_stream", "cfdgpu_set_history",
+    "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
+    "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
+]
+
+OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV = 0, -1, -2, -3, -4, -5, -6
+PC = {"none": 0, "jacobi": 1, "pbjacobi": 2}
+PREC = {"fp64": 0, "mixed": 1}
+MAX_NEWTON = 32
+
+
+class Mesh(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int), ("npElem", ctypes.c_int), ("nNode", ctypes.c_int), ("nElem", ctypes.c_int),
+                ("coords", ctypes.c_void_p), ("conn", ctypes.c_void_p), ("nDBC", ctypes.c_int),
+                ("dbc_node", ctypes.c_void_p), ("dbc_dof", ctypes.c_void_p), ("dbc_value", ctypes.c_void_p)]
+
+
+class Control(ctypes.Structure):
+    _fields_ = [("rho", ctypes.c_double), ("mu", ctypes.c_double), ("bodyforce", ctypes.c_double * 3),
+                ("stab", ctypes.c_double * 3), ("tis", ctypes.c_int), ("rhoInf", ctypes.c_double),
+                ("dt", ctypes.c_double), ("newton_tol", ctypes.c_double), ("newton_max_iter", ctypes.c_int)]
+
+
+class SolverOpts(ctypes.Structure):
+    _fields_ = [("restart", ctypes.c_int), ("rtol", ctypes.c_double), ("atol", ctypes.c_double),
+                ("dtol", ctypes.c_double), ("max_it", ctypes.c_int), ("pc_type", ctypes.c_int),
+                ("precision", ctypes.c_int), ("inner_restart", ctypes.c_int), ("inner_rtol", ctypes.c_double),
+                ("reuse_tangent", ctypes.c_int)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("newton_iters", ctypes.c_int), ("converged", ctypes.c_int),
+                ("norms", ctypes.c_double * MAX_NEWTON), ("ksp_its", ctypes.c_int * MAX_NEWTON),
+                ("ksp_reason", ctypes.c_int * MAX_NEWTON), ("refinements", ctypes.c_int * MAX_NEWTON),
+                ("ms_assembly", ctypes.c_double), ("ms_solver", ctypes.c_double), ("ms_total", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        n = self.newton_iters
+        nsolve = n if not self.converged else n - 1
+        return {"newton_iters": n, "converged": bool(self.converged), "norms": list(self.norms[:n]),
+                "ksp_its": list(self.ksp_its[:nsolve]), "ksp_reason": list(self.ksp_reason[:nsolve]),
+                "refinements": list(self.refinements[:nsolve]), "ms_assembly": self.ms_assembly,
+                "ms_solver": self.ms_solver, "ms_total": self.ms_total}
+
+
+class PatternInfo(ctypes.Structure):
+    _fields_ = [("nNode", ctypes.c_int), ("nElem", ctypes.c_int), ("npElem", ctypes.c_int), ("ndof", ctypes.c_int),
+                ("nnzb", ctypes.c_int64), ("ncolors", ctypes.c_int), ("nfixed", ctypes.c_int), ("nfree", ctypes.c_int)]
+
+
+_LIB: Optional[ctypes.CDLL] = None
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Load libcfdgpu.so (building it with nvcc when absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH) and build_if_missing:
+        from . import build as _build
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"CUDA library not built: {LIB_PATH}")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.cfdgpu_create.argtypes = [ctypes.POINTER(Mesh), ctypes.POINTER(Control), ctypes.POINTER(SolverOpts),
+                                ctypes.POINTER(vp)]
+    L.cfdgpu_destroy.argtypes = [vp]
+    L.cfdgpu_last_error.argtypes = [vp]
+    L.cfdgpu_last_error.restype = ctypes.c_char_p
+    L.cfdgpu_step.argtypes = [vp, dp, dp, ctypes.POINTER(StepStats)]
+    L.cfdgpu_get_solution.argtypes = [vp, vp]
+    L.cfdgpu_set_solution.argtypes = [vp, vp]
+    L.cfdgpu_device_solution.argtypes = [vp, ctypes.POINTER(vp)]
+    L.cfdgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.cfdgpu_set_history.argtypes = [vp, vp, vp]
+    L.cfdgpu_element_matrices.argtypes = [vp, vp, ip, vp, vp]
+    L.cfdgpu_set_element_state.argtypes = [vp, vp, vp, vp]
+    L.cfdgpu_pattern_info_get.argtypes = [vp, ctypes.POINTER(PatternInfo)]
+    L.cfdgpu_export_pattern.argtypes = [vp] + [vp] * 8
+    L.cfdgpu_pattern_build.argtypes = [ctypes.POINTER(Mesh), ctypes.POINTER(PatternInfo)] + [vp] * 8
+    L.cfdgpu_assemble_export.argtypes = [vp, ip, vp, vp]
+    L.cfdgpu_solve_export.argtypes = [vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.cfdgpu_timers.argtypes = [vp, vp]
+    L.cfdgpu_launch_count.argtypes = [vp]
+    L.cfdgpu_launch_count.restype = ctypes.c_int64
+    for name in EXPORTS:
+        if name not in ("cfdgpu_last_error", "cfdgpu_launch_count"):
+            getattr(L, name).restype = ctypes.c_int
+    _LIB = L
+    return L
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+_PATTERN_KEYS = ("rowptr", "colidx", "slot", "color", "color_ptr", "color_elems", "fixed_dofs", "dofmap")
+
+
+def _pattern_arrays(pi) -> dict:
+    return {"rowptr": np.zeros(pi.nNode + 1, np.int32), "colidx": np.zeros(max(pi.nnzb, 1), np.int32),
+            "slot": np.zeros(pi.nElem * pi.npElem * pi.npElem, np.int32), "color": np.zeros(pi.nElem, np.int32),
+            "color_ptr": np.zeros(pi.ncolors + 1, np.int32), "color_elems": np.zeros(pi.nElem, np.int32),
+            "fixed_dofs": np.zeros(max(pi.nfixed, 1), np.int32), "dofmap": np.zeros(pi.nNode * pi.ndof, np.int32)}
+
+
+def _mesh_struct(mesh):
+    """(Mesh struct, keep-alive arrays) for a io.Mesh."""
+    coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+    conn = np.ascontiguousarray(mesh.conn, dtype=np.int32)
+    dn = np.ascontiguousarray(mesh.dbc[:, 0], dtype=np.int32) if mesh.nDBC else np.zeros(1, np.int32)
+    dd = np.ascontiguousarray(mesh.dbc[:, 1], dtype=np.int32) if mesh.nDBC else np.zeros(1, np.int32)
+    dv = np.ascontiguousarray(mesh.dbc[:, 2], dtype=np.float64) if mesh.nDBC else np.zeros(1)
+    m = Mesh(mesh.ndim, mesh.npElem, mesh.nNode, mesh.nElem, _ptr(coords), _ptr(conn), mesh.nDBC, _ptr(dn), _ptr(dd),
+             _ptr(dv))
+    return m, (coords, conn, dn, dd, dv)
+
+
+def pattern_build(mesh) -> dict:
+    """Host-only pattern/colouring/slot-map build (cfdgpu_pattern_build); needs no GPU."""
+    L = load()
+    m, keep = _mesh_struct(mesh)
+    pi = PatternInfo()
+    rc = L.cfdgpu_pattern_build(ctypes.byref(m), ctypes.byref(pi), *([None] * 8))
+    if rc != 0:
+        raise CfdGpuError(rc, "pattern build failed")
+    d = _pattern_arrays(pi)
+    rc = L.cfdgpu_pattern_build(ctypes.byref(m), ctypes.byref(pi), *[_ptr(d[k]) for k in _PATTERN_KEYS])
+    if rc != 0:
+        raise CfdGpuError(rc, "pattern build failed")
+    d["colidx"] = d["colidx"][:pi.nnzb]
+    d["fixed_dofs"] = d["fixed_dofs"][:pi.nfixed]
+    d["info"] = pi
+    return d
+
+
+class CfdGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"cfdgpu error {code}: {msg}")
+        self.code = code
+
+
+class Handle:
+    """Owning wrapper of a cfdgpu_handle."""
+
+    def __init__(self, mesh, ctrl, restart: int = 50, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e4,
+                 max_it: int = 10000, pc: str = "jacobi", precision: str = "fp64", inner_restart: int = 0,
+                 inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
+                 newton_max_iter: int = 10):
+        L = load()
+        self._L = L
+        self.h = ctypes.c_void_p()
+        self.ndim, self.npe = mesh.ndim, mesh.npElem
+        self.ndof = mesh.ndim + 1
+        self.nNode, self.nElem = mesh.nNode, mesh.nElem
+        m, self._keep = _mesh_struct(mesh)
+        c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
+                    ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
+        o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
+                       1 if reuse_tangent else 0)
+        rc = L.cfdgpu_create(ctypes.byref(m), ctypes.byref(c), ctypes.byref(o), ctypes.byref(self.h))
+        if rc != 0:
+            msg = L.cfdgpu_last_error(self.h).decode() if self.h else "create failed"
+            L.cfdgpu_destroy(self.h)
+            self.h = ctypes.c_void_p()
+            raise CfdGpuError(rc, msg)
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise CfdGpuError(rc, self._L.cfdgpu_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            self._L.cfdgpu_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n(self) -> int:
+        return self.nNode * self.ndof
+
+    def step(self, timeNow: float, timeFact: float) -> StepStats:
+        st = StepStats()
+        rc = self._L.cfdgpu_step(self.h, timeNow, timeFact, ctypes.byref(st))
+        if rc != 0:
+            raise CfdGpuError(rc, self._L.cfdgpu_last_error(self.h).decode())
+        return st
+
+    def get_solution(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        out = np.empty(self.n) if out is None else out
+        self._check(self._L.cfdgpu_get_solution(self.h, _ptr(out)))
+        return out
+
+    def set_solution(self, soln: np.ndarray):
+        s = np.ascontiguousarray(soln, dtype=np.float64)
+        self._check(self._L.cfdgpu_set_solution(self.h, _ptr(s)))
+
+    def set_history(self, solnPrev=None, solnDot=None):
+        a = None if solnPrev is None else np.ascontiguousarray(solnPrev, dtype=np.float64)
+        b = None if solnDot is None else np.ascontiguousarray(solnDot, dtype=np.float64)
+        self._check(self._L.cfdgpu_set_history(self.h, _ptr(a), _ptr(b)))
+
+    def stream_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(self._L.cfdgpu_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def device_solution_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(self._L.cfdgpu_device_solution(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def set_element_state(self, prev, cur, dotcur):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (prev, cur, dotcur)]
+        self._check(self._L.cfdgpu_set_element_state(self.h, *[_ptr(a) for a in arrs]))
+
+    def element_matrices(self, elem_ids):
+        ids = np.ascontiguousarray(elem_ids, dtype=np.int32)
+        nsize = self.npe * self.ndof
+        K = np.zeros((len(ids), nsize, nsize))
+        F = np.zeros((len(ids), nsize))
+        self._check(self._L.cfdgpu_element_matrices(self.h, _ptr(ids), len(ids), _ptr(K), _ptr(F)))
+        return K, F
+
+    def pattern_info(self) -> PatternInfo:
+        pi = PatternInfo()
+        self._check(self._L.cfdgpu_pattern_info_get(self.h, ctypes.byref(pi)))
+        return pi
+
+    def export_pattern(self) -> dict:
+        pi = self.pattern_info()
+        d = _pattern_arrays(pi)
+        self._check(self._L.cfdgpu_export_pattern(self.h, *[_ptr(d[k]) for k in _PATTERN_KEYS]))
+        d["colidx"] = d["colidx"][:pi.nnzb]
+        d["fixed_dofs"] = d["fixed_dofs"][:pi.nfixed]
+        d["info"] = pi
+        return d
+
+    def assemble_export(self, it: int = 0):
+        pi = self.pattern_info()
+        vals = np.zeros(pi.nnzb * pi.ndof * pi.ndof)
+        rhs = np.zeros(self.n)
+        self._check(self._L.cfdgpu_assemble_export(self.h, it, _ptr(vals), _ptr(rhs)))
+        return vals.reshape(pi.nnzb, pi.ndof, pi.ndof), rhs
+
+    def solve_export(self, b: np.ndarray):
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        its, reason = ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.cfdgpu_solve_export(self.h, _ptr(bb), _ptr(x), ctypes.byref(its), ctypes.byref(reason)))
+        return x, its.value, reason.value
+
+    def timers(self) -> np.ndarray:
+        t = np.zeros(5)
+        self._check(self._L.cfdgpu_timers(self.h, _ptr(t)))
+        return t
+
+    def launch_count(self) -> int:
+        return int(self._L.cfdgpu_launch_count(self.h))

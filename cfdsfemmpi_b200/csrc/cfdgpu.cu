@@ -1,0 +1,769 @@
+// cfdgpu.cu -- host side of the C ABI declared in include/cfdgpu.h.
+//
+// Device layout (all resident in HBM for the handle's lifetime):
+//   coords   nNode*ndim FP64, conn nElem*npe int32 (element-major)
+//   nodal vectors (nNode*ndof FP64, reference layout node*ndof+dof):
+//     soln, solnPrev, solnPrev2..4, solnCur, solnDot, solnDotPrev, solnDotCur,
+//     solnApplied, rhs, dx
+//   BSR: rowptr (nNode+1), colidx (nnzb), values nnzb*ndof*ndof (row-major
+//     blocks, FP64; FP32 copy in mixed mode), diag_slot per node
+//   element->block slot map nElem*npe*npe int32, colour-ordered element list
+//   Krylov basis (m+1) vectors, Hessenberg/Givens arrays, reduction scratch
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cfdgpu.h"
+#include "element_kernels.cuh"
+#include "linalg_kernels.cuh"
+#include "setup.h"
+
+using namespace cfdgpu;
+
+namespace {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct cfdgpu_handle {
+  std::string err;
+  int ndim = 0, npe = 0, ndof = 0, nNode = 0, nElem = 0, et = 0;
+  int64_t n = 0;  // nNode*ndof
+  cfdgpu_control ctrl{};
+  cfdgpu_solver_opts opts{};
+  Topology topo;
+  double td[16] = {0};
+  bool td_set = false;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> allocs;
+  int64_t launches = 0;
+  double timers[5] = {0, 0, 0, 0, 0};
+
+  // device arrays
+  double *coords = nullptr;
+  int32_t *conn = nullptr;
+  int32_t *rowptr = nullptr, *colidx = nullptr, *slot = nullptr, *color_elems = nullptr, *diag_slot = nullptr;
+  uint8_t *fixmask = nullptr;
+  int32_t *dbc_index = nullptr, *fixed_dofs = nullptr, *dbc_mult = nullptr;
+  double *dbc_value = nullptr;
+  double *soln = nullptr, *prev = nullptr, *prev2 = nullptr, *prev3 = nullptr, *prev4 = nullptr;
+  double *cur = nullptr, *dot = nullptr, *dotPrev = nullptr, *dotCur = nullptr, *applied = nullptr;
+  double *rhs = nullptr, *dx = nullptr;
+  double *bsr = nullptr;
+  double *dinv = nullptr, *binv = nullptr;
+  int m = 0;
+  double *V = nullptr;
+  GmresState *gst = nullptr;
+  GmresArrays ga{};
+  double *red_partial = nullptr;
+  unsigned int *red_counter = nullptr;
+  double *scalar = nullptr;          // device scalar slots
+  int *negjac = nullptr;
+  double *h_scalar = nullptr;        // pinned host mirror
+  GmresState *h_gst = nullptr;       // pinned
+  bool assembled_K = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+      return CFDGPU_ECUDA;                                                         \
+    }                                                                              \
+  } while (0)
+
+#define LAUNCHED(h) ((h)->launches++)
+
+static int check_launch(cfdgpu_handle *h, const char *what)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    h->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return CFDGPU_ECUDA;
+  }
+  return 0;
+}
+
+template <typename T>
+static int dalloc(cfdgpu_handle *h, T **p, size_t count)
+{
+  void *q = nullptr;
+  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
+    return CFDGPU_ENOMEM;
+  }
+  h->allocs.push_back(q);
+  *p = (T *)q;
+  return 0;
+}
+
+template <typename T>
+static int upload(cfdgpu_handle *h, T **p, const T *src, size_t count)
+{
+  int rc = dalloc(h, p, count);
+  if (rc) return rc;
+  if (count) CK(cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// SetTimeParametersFluid (src/base/UtilitiesGeneral.cpp:5-205)
+static void time_params(int tis, double rho, double dt, double *td)
+{
+  for (int i = 0; i < 16; i++) td[i] = 0.0;
+  td[0] = dt;
+  double alpf, alpm, gamm;
+  switch (tis) {
+    case 0:
+      td[1] = 1.0; td[2] = 1.0; td[3] = 1.0; td[4] = 1.0;
+      break;
+    case 1:
+      alpf = 1.0 / (1.0 + rho); alpm = 1.0; gamm = 1.0;
+      td[1] = alpm; td[2] = alpf; td[3] = alpm; td[4] = gamm;
+      td[5] = alpf * dt; td[6] = alpm / gamm; td[7] = 1.0 - alpm / gamm; td[8] = 0.0;
+      td[9] = 1.0 / dt; td[10] = -td[9];
+      break;
+    case 2:
+    case 4:
+      alpf = 1.0 / (1.0 + rho); alpm = 0.5 * (3.0 - rho) / (1.0 + rho); gamm = 0.5 + alpm - alpf;
+      td[1] = alpm; td[2] = alpf; td[3] = alpm; td[4] = gamm;
+      td[5] = alpf * dt; td[6] = alpm / gamm; td[7] = 1.0 - alpm / gamm; td[8] = alpm / gamm / dt;
+      td[9] = 1.0 / gamm / dt; td[10] = -td[9]; td[15] = 1.0 - 1.0 / gamm;
+      break;
+    case 3:
+    case 5:
+    case 6:
+    case 7: {
+      td[1] = 1.0; td[2] = 1.0; td[3] = 1.0; td[4] = 1.0;
+      td[5] = dt; td[6] = 1.0; td[7] = 0.0; td[8] = 1.0 / dt;
+      if (tis == 3) { td[9] = 1.0 / dt; td[10] = -1.0 / dt; }
+      if (tis == 5) { td[9] = 1.5 / dt; td[10] = -2.0 / dt; td[11] = 0.5 / dt; }
+      if (tis == 6) { td[9] = (11.0 / 6.0) / dt; td[10] = -3.0 / dt; td[11] = 1.5 / dt; td[12] = -(1.0 / 3.0) / dt; }
+      if (tis == 7) {
+        td[9] = (25.0 / 12.0) / dt; td[10] = -4.0 / dt; td[11] = 3.0 / dt; td[12] = -(4.0 / 3.0) / dt;
+        td[13] = (1.0 / 4.0) / dt;
+      }
+    } break;
+    default:
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// small elementwise kernels
+
+struct TdCoef {
+  double c9, c10, c11, c12, c13, c15, af, am;
+};
+
+// SolutionData::updateIterStep (src/base/SolutionData.cpp:83-91)
+__global__ void k_update_iter_step(int64_t n, TdCoef c, const double *__restrict__ soln,
+                                   const double *__restrict__ prev, const double *__restrict__ prev2,
+                                   const double *__restrict__ prev3, const double *__restrict__ prev4,
+                                   const double *__restrict__ dotPrev, double *__restrict__ dot,
+                                   double *__restrict__ cur, double *__restrict__ dotCur)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double s = soln[i], p = prev[i], dp = dotPrev[i];
+    const double d = c.c9 * s + c.c10 * p + c.c11 * prev2[i] + c.c12 * prev3[i] + c.c13 * prev4[i] + c.c15 * dp;
+    dot[i] = d;
+    cur[i] = c.af * s + (1.0 - c.af) * p;
+    dotCur[i] = c.am * d + (1.0 - c.am) * dp;
+  }
+}
+
+// StabFEM::assignBoundaryConditions (src/base/StabFEM.cpp:391-410)
+__global__ void k_apply_bc(int nDBC, const int32_t *__restrict__ idx, const double *__restrict__ val,
+                           double timeFact, const double *__restrict__ soln, double *__restrict__ applied)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nDBC) applied[idx[k]] = val[k] * timeFact - soln[idx[k]];
+}
+
+// soln[d] += solnApplied[d], once per Dirichlet entry naming d (StabFEM2.cpp:719-730)
+__global__ void k_dirichlet_update(int nfix, const int32_t *__restrict__ fixed, const int32_t *__restrict__ mult,
+                                   const double *__restrict__ applied, double *__restrict__ soln)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nfix) return;
+  const int32_t g = fixed[k];
+  double s = soln[g];
+  const double a = applied[g];
+  for (int r = 0; r < mult[k]; r++) s += a;
+  soln[g] = s;
+}
+
+// identity on the diagonal of prescribed dofs
+template <typename VT>
+__global__ void k_dirichlet_diag(int nfix, int ndof, const int32_t *__restrict__ fixed,
+                                 const int32_t *__restrict__ diag_slot, VT *__restrict__ bsr)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nfix) return;
+  const int32_t g = fixed[k];
+  const int node = g / ndof, d = g % ndof;
+  bsr[(int64_t)diag_slot[node] * ndof * ndof + d * ndof + d] = VT(1);
+}
+
+__global__ void k_axpy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ y)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+
+static inline int grid_for(int64_t n, int bs = 256, int cap = 148 * 16)
+{
+  int64_t g = (n + bs - 1) / bs;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------------------
+// element launches
+
+template <int ET, int MODE, bool LIFT>
+static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, double *outK, double *outF)
+{
+  constexpr int GS = ElemTraits<ET>::GS;
+  constexpr int GROUPS = (GS == 32) ? 4 : 8;
+  const int grid = (nel + GROUPS - 1) / GROUPS;
+  if (grid <= 0) return 0;
+  ElemParams P;
+  P.rho = h->ctrl.rho; P.mu = h->ctrl.mu; P.af = h->td[2]; P.am = h->td[1]; P.acceFact = h->td[8];
+  P.stab0 = h->ctrl.stab[0]; P.stab1 = h->ctrl.stab[1]; P.stab2 = h->ctrl.stab[2];
+  element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+      elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
+      h->rhs, outK, outF, h->negjac);
+  LAUNCHED(h);
+  return check_launch(h, "element_kernel");
+}
+
+template <int MODE, bool LIFT>
+static int launch_elements_et(cfdgpu_handle *h, const int32_t *elems, int nel, double *outK, double *outF)
+{
+  switch (h->et) {
+    case CFDGPU_HEX8: return launch_elements<CFDGPU_HEX8, MODE, LIFT>(h, elems, nel, outK, outF);
+    case CFDGPU_TET4: return launch_elements<CFDGPU_TET4, MODE, LIFT>(h, elems, nel, outK, outF);
+    case CFDGPU_QUAD4: return launch_elements<CFDGPU_QUAD4, MODE, LIFT>(h, elems, nel, outK, outF);
+    default: return launch_elements<CFDGPU_TRI3, MODE, LIFT>(h, elems, nel, outK, outF);
+  }
+}
+
+// Assembly of one Newton iteration: rhs (and the tangent when want_K),
+// colour by colour (StabFEM2.cpp:658-738).
+static int assemble(cfdgpu_handle *h, int iter, bool want_K)
+{
+  CK(cudaMemsetAsync(h->rhs, 0, sizeof(double) * h->n, h->stream));
+  const Topology &t = h->topo;
+  for (int c = 0; c < t.ncolors; c++) {
+    const int32_t *el = h->color_elems + t.color_ptr[c];
+    const int nel = t.color_ptr[c + 1] - t.color_ptr[c];
+    int rc;
+    if (want_K) {
+      rc = (iter == 0) ? launch_elements_et<MODE_ASSEMBLE, true>(h, el, nel, nullptr, nullptr)
+                       : launch_elements_et<MODE_ASSEMBLE, false>(h, el, nel, nullptr, nullptr);
+    } else {
+      rc = (iter == 0) ? launch_elements_et<MODE_RESIDUAL, true>(h, el, nel, nullptr, nullptr)
+                       : launch_elements_et<MODE_RESIDUAL, false>(h, el, nel, nullptr, nullptr);
+    }
+    if (rc) return rc;
+  }
+  if (want_K && !t.fixed_dofs.empty()) {
+    const int nfix = (int)t.fixed_dofs.size();
+    k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
+    LAUNCHED(h);
+    int rc = check_launch(h, "dirichlet_diag");
+    if (rc) return rc;
+    h->assembled_K = true;
+  }
+  return 0;
+}
+
+static int build_pc(cfdgpu_handle *h)
+{
+  const int pc = h->opts.pc_type;
+  if (pc == CFDGPU_PC_NONE) return 0;
+  const int g = (h->nNode + 127) / 128;
+  if (h->ndof == 4) build_jacobi<4, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
+  else build_jacobi<3, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
+  LAUNCHED(h);
+  return check_launch(h, "build_jacobi");
+}
+
+// y = M^-1 (A x) (mode 0) or y = M^-1 (b - A x) (mode 1)
+static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y, const GmresState *st, int j)
+{
+  const int pc = h->opts.pc_type;
+  if (h->ndof == 4) {
+    const int grid = (int)((h->nNode * 32LL + 255) / 256);
+#define SPMV4(MO, PCV)                                                                                  \
+  bsr4_spmv_f64<MO, PCV><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, h->dinv, \
+                                                       h->binv, y, st, j)
+    if (mode == 0) {
+      if (pc == 0) SPMV4(0, 0); else if (pc == 1) SPMV4(0, 1); else SPMV4(0, 2);
+    } else {
+      if (pc == 0) SPMV4(1, 0); else if (pc == 1) SPMV4(1, 1); else SPMV4(1, 2);
+    }
+#undef SPMV4
+  } else {
+    const int grid = (int)((h->n + 255) / 256);
+#define SPMV3(MO, PCV)                                                                                        \
+  bsr_spmv_generic<3, MO, PCV, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, \
+                                                                     h->dinv, h->binv, y, st, j)
+    if (mode == 0) {
+      if (pc == 0) SPMV3(0, 0); else if (pc == 1) SPMV3(0, 1); else SPMV3(0, 2);
+    } else {
+      if (pc == 0) SPMV3(1, 0); else if (pc == 1) SPMV3(1, 1); else SPMV3(1, 2);
+    }
+#undef SPMV3
+  }
+  LAUNCHED(h);
+  return check_launch(h, "bsr_spmv");
+}
+
+static int norm2(cfdgpu_handle *h, const double *x, double *out_host)
+{
+  norm2_kernel<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(h->n, x, h->red_partial, h->red_counter, h->scalar);
+  LAUNCHED(h);
+  int rc = check_launch(h, "norm2");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->h_scalar, h->scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *out_host = h->h_scalar[0];
+  return 0;
+}
+
+// Restarted GMRES on the assembled BSR: x = A^-1 b, x0 = 0.
+static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+{
+  const int64_t n = h->n;
+  const int m = h->m;
+  const int64_t ldv = n;
+  double *V = h->V;
+  GmresState *st = h->gst;
+  int rc;
+  gmres_init<<<1, 1, 0, h->stream>>>(st, m, h->opts.max_it, h->opts.rtol, h->opts.atol, h->opts.dtol);
+  LAUNCHED(h);
+  CK(cudaMemsetAsync(x, 0, sizeof(double) * n, h->stream));
+  // V0 = M^-1 b (x0 = 0)
+  if (h->ndof == 4) pc_apply<4><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, V);
+  else pc_apply<3><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, V);
+  LAUNCHED(h);
+  const int vgrid = grid_for(n);
+  while (true) {
+    gmres_start<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, st, h->ga);
+    scale_v0<<<vgrid, 256, 0, h->stream>>>(n, V, st);
+    h->launches += 2;
+    if ((rc = check_launch(h, "gmres_start"))) return rc;
+    // Arnoldi steps; poll the device flag one chunk behind so the GPU stays fed
+    const int CH = 8;
+    bool stop = false;
+    int polled_chunk = -1;
+    cudaEvent_t evs[2] = {h->ev0, h->ev1};
+    for (int j0 = 0; j0 < m && !stop; j0 += CH) {
+      for (int j = j0; j < std::min(m, j0 + CH); j++) {
+        if ((rc = spmv_pc(h, 0, V + (int64_t)j * ldv, nullptr, V + (int64_t)(j + 1) * ldv, st, j))) return rc;
+        dim3 g2(RED_BLOCKS, (j + 1 + MDOT_CHUNK - 1) / MDOT_CHUNK);
+        gmres_mdot<<<g2, RED_THREADS, 0, h->stream>>>(n, V, ldv, j, st, h->ga);
+        gmres_maxpy_norm<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, ldv, j, st, h->ga);
+        gmres_scale_next<<<vgrid, 256, 0, h->stream>>>(n, V, ldv, j, st);
+        h->launches += 3;
+      }
+      if ((rc = check_launch(h, "gmres_arnoldi"))) return rc;
+      const int cidx = (j0 / CH) & 1;
+      CK(cudaMemcpyAsync(&h->h_gst[cidx], st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaEventRecord(evs[cidx], h->stream));
+      // wait for the previous chunk's snapshot
+      if (polled_chunk >= 0 || j0 > 0) {
+        const int pidx = ((j0 / CH) - 1) & 1;
+        if (j0 > 0) {
+          CK(cudaEventSynchronize(evs[pidx]));
+          if (!h->h_gst[pidx].active) stop = true;
+        }
+      }
+      polled_chunk = j0 / CH;
+    }
+    gmres_backsub<<<1, 32, 0, h->stream>>>(st, h->ga);
+    gmres_update_x<<<vgrid, 256, 0, h->stream>>>(n, x, V, ldv, st, h->ga);
+    h->launches += 2;
+    if ((rc = check_launch(h, "gmres_build_soln"))) return rc;
+    CK(cudaMemcpyAsync(h->h_gst, st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    GmresState s = h->h_gst[0];
+    int reason = s.reason;
+    if (reason == 0 && s.its >= h->opts.max_it) reason = -3;   // KSP_DIVERGED_ITS
+    if (reason != 0) {
+      if (its_out) *its_out = s.its;
+      if (reason_out) *reason_out = reason;
+      return 0;
+    }
+    // restart: V0 = M^-1 (b - A x)
+    if ((rc = spmv_pc(h, 1, x, b, V, nullptr, 0))) return rc;
+  }
+}
+
+static int upload_td(cfdgpu_handle *h)
+{
+  time_params(h->ctrl.tis, h->ctrl.rhoInf, h->ctrl.dt, h->td);
+  h->td_set = true;
+  return 0;
+}
+
+static int update_iter_step(cfdgpu_handle *h)
+{
+  TdCoef c{h->td[9], h->td[10], h->td[11], h->td[12], h->td[13], h->td[15], h->td[2], h->td[1]};
+  k_update_iter_step<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, c, h->soln, h->prev, h->prev2, h->prev3, h->prev4,
+                                                            h->dotPrev, h->dot, h->cur, h->dotCur);
+  LAUNCHED(h);
+  return check_launch(h, "update_iter_step");
+}
+
+static int check_negjac(cfdgpu_handle *h)
+{
+  int v = 0;
+  CK(cudaMemcpyAsync(&v, h->negjac, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (v) {
+    h->err = "Negative Jacobian in the element routine";
+    return CFDGPU_ENEGJAC;
+  }
+  return 0;
+}
+
+extern "C" {
+
+int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfdgpu_solver_opts *opts,
+                  cfdgpu_handle **out)
+{
+  if (!out) return CFDGPU_EINVAL;
+  *out = nullptr;
+  cfdgpu_handle *h = new cfdgpu_handle();
+  *out = h;
+  if (!mesh || !ctrl || !opts || !mesh->coords || !mesh->conn) { h->err = "null argument"; return CFDGPU_EINVAL; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { h->err = "no CUDA device"; return CFDGPU_ENODEV; }
+  h->ndim = mesh->ndim; h->npe = mesh->npElem; h->ndof = mesh->ndim + 1;
+  h->nNode = mesh->nNode; h->nElem = mesh->nElem;
+  if (h->ndim == 2 && h->npe == 3) h->et = CFDGPU_TRI3;
+  else if (h->ndim == 2 && h->npe == 4) h->et = CFDGPU_QUAD4;
+  else if (h->ndim == 3 && h->npe == 4) h->et = CFDGPU_TET4;
+  else if (h->ndim == 3 && h->npe == 8) h->et = CFDGPU_HEX8;
+  else { h->err = " Invalid npElem " + std::to_string(h->npe); return CFDGPU_EINVAL; }
+  h->n = (int64_t)h->nNode * h->ndof;
+  h->ctrl = *ctrl;
+  h->opts = *opts;
+  if (h->opts.restart <= 0) h->opts.restart = 30;
+  if (h->opts.restart > 1000) { h->err = "restart > 1000 is not supported"; return CFDGPU_EINVAL; }
+  if (h->opts.max_it <= 0) h->opts.max_it = 10000;
+  if (h->ctrl.newton_max_iter <= 0) h->ctrl.newton_max_iter = 10;
+  if (h->ctrl.newton_max_iter > CFDGPU_MAX_NEWTON) h->ctrl.newton_max_iter = CFDGPU_MAX_NEWTON;
+  h->m = h->opts.restart;
+
+  auto t0 = std::chrono::steady_clock::now();
+  std::string msg = build_topology(h->nNode, h->nElem, h->npe, h->ndof, mesh->conn, mesh->nDBC, mesh->dbc_node,
+                                   mesh->dbc_dof, mesh->dbc_value, h->topo);
+  if (!msg.empty()) { h->err = msg; return CFDGPU_EINVAL; }
+  const Topology &t = h->topo;
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&h->ev0, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev1, cudaEventDisableTiming));
+  int rc = 0;
+  const int64_t n = h->n;
+  std::vector<int32_t> diag(h->nNode);
+  for (int v = 0; v < h->nNode; v++) {
+    const int32_t *b = t.colidx.data() + t.rowptr[v], *e = t.colidx.data() + t.rowptr[v + 1];
+    diag[v] = (int32_t)(std::lower_bound(b, e, v) - t.colidx.data());
+  }
+  if ((rc = upload(h, &h->coords, mesh->coords, (size_t)h->nNode * h->ndim))) return rc;
+  if ((rc = upload(h, &h->conn, mesh->conn, (size_t)h->nElem * h->npe))) return rc;
+  if ((rc = upload(h, &h->rowptr, t.rowptr.data(), t.rowptr.size()))) return rc;
+  if ((rc = upload(h, &h->colidx, t.colidx.data(), t.colidx.size()))) return rc;
+  if ((rc = upload(h, &h->slot, t.slot.data(), t.slot.size()))) return rc;
+  if ((rc = upload(h, &h->color_elems, t.color_elems.data(), t.color_elems.size()))) return rc;
+  if ((rc = upload(h, &h->diag_slot, diag.data(), diag.size()))) return rc;
+  if ((rc = upload(h, &h->fixmask, t.fixmask.data(), t.fixmask.size()))) return rc;
+  if ((rc = upload(h, &h->dbc_index, t.dbc_index.data(), t.dbc_index.size()))) return rc;
+  if ((rc = upload(h, &h->dbc_value, t.dbc_value.data(), t.dbc_value.size()))) return rc;
+  if ((rc = upload(h, &h->fixed_dofs, t.fixed_dofs.data(), t.fixed_dofs.size()))) return rc;
+  if ((rc = upload(h, &h->dbc_mult, t.dbc_mult.data(), t.dbc_mult.size()))) return rc;
+  double **vecs[] = {&h->soln, &h->prev, &h->prev2, &h->prev3, &h->prev4, &h->cur, &h->dot,
+                     &h->dotPrev, &h->dotCur, &h->applied, &h->rhs, &h->dx};
+  for (double **v : vecs) {
+    if ((rc = dalloc(h, v, (size_t)n))) return rc;
+    CK(cudaMemset(*v, 0, sizeof(double) * n));
+  }
+  const size_t bb = (size_t)h->ndof * h->ndof;
+  if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
+  CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
+  if ((rc = dalloc(h, &h->dinv, (size_t)n))) return rc;
+  if ((rc = dalloc(h, &h->binv, (size_t)h->nNode * bb))) return rc;
+  if ((rc = dalloc(h, &h->V, (size_t)n * (h->m + 1)))) return rc;
+  if ((rc = dalloc(h, &h->gst, 1))) return rc;
+  if ((rc = dalloc(h, &h->ga.H, (size_t)(h->m + 1) * h->m))) return rc;
+  if ((rc = dalloc(h, &h->ga.cs, (size_t)h->m))) return rc;
+  if ((rc = dalloc(h, &h->ga.sn, (size_t)h->m))) return rc;
+  if ((rc = dalloc(h, &h->ga.grs, (size_t)h->m + 1))) return rc;
+  if ((rc = dalloc(h, &h->ga.y, (size_t)h->m))) return rc;
+  if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * RED_BLOCKS))) return rc;
+  if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
+  if ((rc = dalloc(h, &h->red_counter, 1))) return rc;
+  CK(cudaMemset(h->red_counter, 0, sizeof(unsigned int)));
+  if ((rc = dalloc(h, &h->scalar, 8))) return rc;
+  if ((rc = dalloc(h, &h->negjac, 1))) return rc;
+  CK(cudaMemset(h->negjac, 0, sizeof(int)));
+  CK(cudaMemset(h->gst, 0, sizeof(GmresState)));
+  CK(cudaMallocHost(&h->h_scalar, 8 * sizeof(double)));
+  CK(cudaMallocHost(&h->h_gst, 2 * sizeof(GmresState)));
+  CK(cudaDeviceSynchronize());
+  h->timers[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return 0;
+}
+
+int cfdgpu_destroy(cfdgpu_handle *h)
+{
+  if (!h) return 0;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->h_scalar) cudaFreeHost(h->h_scalar);
+  if (h->h_gst) cudaFreeHost(h->h_gst);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return 0;
+}
+
+const char *cfdgpu_last_error(const cfdgpu_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_stats *stats)
+{
+  (void)timeNow;
+  if (!h || !stats) return CFDGPU_EINVAL;
+  memset(stats, 0, sizeof(*stats));
+  auto tstart = std::chrono::steady_clock::now();
+  int rc;
+  upload_td(h);
+  // SolutionData::timeUpdate (SolutionData.cpp:64-78): rotate history
+  double *old4 = h->prev4;
+  h->prev4 = h->prev3; h->prev3 = h->prev2; h->prev2 = h->prev; h->prev = old4;
+  CK(cudaMemcpyAsync(h->prev, h->soln, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->dotPrev, h->dot, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+  const int nDBC = (int)h->topo.dbc_index.size();
+  if (nDBC) {
+    k_apply_bc<<<(nDBC + 255) / 256, 256, 0, h->stream>>>(nDBC, h->dbc_index, h->dbc_value, timeFact, h->soln, h->applied);
+    LAUNCHED(h);
+    if ((rc = check_launch(h, "apply_bc"))) return rc;
+  }
+  const int nfix = (int)h->topo.fixed_dofs.size();
+  const bool reuse = h->opts.reuse_tangent != 0;
+  double ms_asm = 0.0, ms_sol = 0.0;
+  for (int iter = 0; iter < h->ctrl.newton_max_iter; iter++) {
+    auto ta = std::chrono::steady_clock::now();
+    if ((rc = update_iter_step(h))) return rc;
+    const bool want_K = !reuse || iter == 0;
+    if ((rc = assemble(h, iter, want_K))) return rc;
+    if (iter == 0 && nfix) {
+      k_dirichlet_update<<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->fixed_dofs, h->dbc_mult, h->applied, h->soln);
+      LAUNCHED(h);
+      if ((rc = check_launch(h, "dirichlet_update"))) return rc;
+    }
+    double norm = 0.0;
+    if ((rc = norm2(h, h->rhs, &norm))) return rc;
+    if ((rc = check_negjac(h))) return rc;
+    ms_asm += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
+    stats->norms[iter] = norm;
+    stats->newton_iters = iter + 1;
+    if (norm < h->ctrl.newton_tol) { stats->converged = 1; break; }
+    auto ts = std::chrono::steady_clock::now();
+    if (want_K && (rc = build_pc(h))) return rc;
+    int its = 0, reason = 0;
+    if ((rc = gmres(h, h->rhs, h->dx, &its, &reason))) return rc;
+    stats->ksp_its[iter] = its;
+    stats->ksp_reason[iter] = reason;
+    if (reason < 0) {
+      h->err = "KSP diverged, reason " + std::to_string(reason) + " after " + std::to_string(its) + " iterations";
+      return CFDGPU_EKSP;
+    }
+    k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0, h->dx, h->soln);
+    LAUNCHED(h);
+    if ((rc = check_launch(h, "axpy"))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    ms_sol += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  stats->ms_assembly = ms_asm;
+  stats->ms_solver = ms_sol;
+  stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tstart).count();
+  h->timers[1] += ms_asm * 1e-3;
+  h->timers[2] += ms_sol * 1e-3;
+  h->timers[4] += stats->ms_total * 1e-3;
+  return 0;
+}
+
+int cfdgpu_get_solution(cfdgpu_handle *h, double *soln)
+{
+  if (!h || !soln) return CFDGPU_EINVAL;
+  CK(cudaMemcpyAsync(soln, h->soln, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int cfdgpu_set_solution(cfdgpu_handle *h, const double *soln)
+{
+  if (!h || !soln) return CFDGPU_EINVAL;
+  CK(cudaMemcpyAsync(h->soln, soln, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int cfdgpu_device_solution(cfdgpu_handle *h, double **dptr)
+{
+  if (!h || !dptr) return CFDGPU_EINVAL;
+  *dptr = h->soln;
+  return 0;
+}
+
+int cfdgpu_stream(cfdgpu_handle *h, void **stream)
+{
+  if (!h || !stream) return CFDGPU_EINVAL;
+  *stream = (void *)h->stream;
+  return 0;
+}
+
+int cfdgpu_set_history(cfdgpu_handle *h, const double *solnPrev, const double *solnDot)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (solnPrev) CK(cudaMemcpyAsync(h->prev, solnPrev, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  if (solnDot) CK(cudaMemcpyAsync(h->dot, solnDot, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int cfdgpu_set_element_state(cfdgpu_handle *h, const double *solnPrev, const double *solnCur, const double *solnDotCur)
+{
+  if (!h) return CFDGPU_EINVAL;
+  upload_td(h);
+  if (solnPrev) CK(cudaMemcpyAsync(h->prev, solnPrev, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  if (solnCur) CK(cudaMemcpyAsync(h->cur, solnCur, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  if (solnDotCur) CK(cudaMemcpyAsync(h->dotCur, solnDotCur, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int cfdgpu_element_matrices(cfdgpu_handle *h, const int32_t *elem_ids, int n, double *K, double *F)
+{
+  if (!h || !elem_ids || n < 0 || !K || !F) return CFDGPU_EINVAL;
+  if (n == 0) return 0;
+  for (int i = 0; i < n; i++)
+    if (elem_ids[i] < 0 || elem_ids[i] >= h->nElem) { h->err = "element id out of range"; return CFDGPU_EINVAL; }
+  if (!h->td_set) upload_td(h);
+  const int nsize = h->npe * h->ndof;
+  int32_t *d_ids = nullptr;
+  double *dK = nullptr, *dF = nullptr;
+  CK(cudaMalloc(&d_ids, sizeof(int32_t) * n));
+  CK(cudaMalloc(&dK, sizeof(double) * (size_t)n * nsize * nsize));
+  CK(cudaMalloc(&dF, sizeof(double) * (size_t)n * nsize));
+  CK(cudaMemcpyAsync(d_ids, elem_ids, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->stream));
+  int rc = launch_elements_et<MODE_EXPORT, false>(h, d_ids, n, dK, dF);
+  if (!rc) {
+    CK(cudaMemcpyAsync(K, dK, sizeof(double) * (size_t)n * nsize * nsize, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(F, dF, sizeof(double) * (size_t)n * nsize, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  cudaFree(d_ids); cudaFree(dK); cudaFree(dF);
+  if (!rc) rc = check_negjac(h);
+  return rc;
+}
+
+int cfdgpu_pattern_info_get(cfdgpu_handle *h, cfdgpu_pattern_info *info)
+{
+  if (!h || !info) return CFDGPU_EINVAL;
+  info->nNode = h->nNode; info->nElem = h->nElem; info->npElem = h->npe; info->ndof = h->ndof;
+  info->nnzb = h->topo.nnzb(); info->ncolors = h->topo.ncolors;
+  info->nfixed = (int)h->topo.fixed_dofs.size(); info->nfree = h->topo.nfree;
+  return 0;
+}
+
+int cfdgpu_export_pattern(cfdgpu_handle *h, int32_t *rowptr, int32_t *colidx, int32_t *slot, int32_t *color,
+                          int32_t *color_ptr, int32_t *color_elems, int32_t *fixed_dofs, int32_t *dofmap)
+{
+  if (!h) return CFDGPU_EINVAL;
+  const Topology &t = h->topo;
+  auto cp = [](int32_t *dst, const std::vector<int32_t> &v) { if (dst && !v.empty()) memcpy(dst, v.data(), v.size() * 4); };
+  cp(rowptr, t.rowptr); cp(colidx, t.colidx); cp(slot, t.slot); cp(color, t.color); cp(color_ptr, t.color_ptr);
+  cp(color_elems, t.color_elems); cp(fixed_dofs, t.fixed_dofs); cp(dofmap, t.dofmap);
+  return 0;
+}
+
+int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int32_t *rowptr, int32_t *colidx,
+                         int32_t *slot, int32_t *color, int32_t *color_ptr, int32_t *color_elems,
+                         int32_t *fixed_dofs, int32_t *dofmap)
+{
+  if (!mesh || !info || !mesh->conn) return CFDGPU_EINVAL;
+  Topology t;
+  std::string msg = build_topology(mesh->nNode, mesh->nElem, mesh->npElem, mesh->ndim + 1, mesh->conn, mesh->nDBC,
+                                   mesh->dbc_node, mesh->dbc_dof, mesh->dbc_value, t);
+  if (!msg.empty()) return CFDGPU_EINVAL;
+  info->nNode = mesh->nNode; info->nElem = mesh->nElem; info->npElem = mesh->npElem; info->ndof = mesh->ndim + 1;
+  info->nnzb = t.nnzb(); info->ncolors = t.ncolors;
+  info->nfixed = (int)t.fixed_dofs.size(); info->nfree = t.nfree;
+  auto cp = [](int32_t *dst, const std::vector<int32_t> &v) { if (dst && !v.empty()) memcpy(dst, v.data(), v.size() * 4); };
+  cp(rowptr, t.rowptr); cp(colidx, t.colidx); cp(slot, t.slot); cp(color, t.color); cp(color_ptr, t.color_ptr);
+  cp(color_elems, t.color_elems); cp(fixed_dofs, t.fixed_dofs); cp(dofmap, t.dofmap);
+  return 0;
+}
+
+int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double *rhs)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (!h->td_set) upload_td(h);
+  int rc = assemble(h, iter, true);
+  if (rc) return rc;
+  const size_t bb = (size_t)h->ndof * h->ndof;
+  if (bsr_vals) CK(cudaMemcpyAsync(bsr_vals, h->bsr, sizeof(double) * h->topo.nnzb() * bb, cudaMemcpyDeviceToHost, h->stream));
+  if (rhs) CK(cudaMemcpyAsync(rhs, h->rhs, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_negjac(h);
+}
+
+int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, int *reason)
+{
+  if (!h || !b || !x) return CFDGPU_EINVAL;
+  if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
+  CK(cudaMemcpyAsync(h->rhs, b, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  int rc = build_pc(h);
+  if (rc) return rc;
+  int i = 0, r = 0;
+  rc = gmres(h, h->rhs, h->dx, &i, &r);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(x, h->dx, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (its) *its = i;
+  if (reason) *reason = r;
+  return 0;
+}
+
+int cfdgpu_timers(cfdgpu_handle *h, double t[5])
+{
+  if (!h || !t) return CFDGPU_EINVAL;
+  for (int i = 0; i < 5; i++) t[i] = h->timers[i];
+  return 0;
+}
+
+int64_t cfdgpu_launch_count(cfdgpu_handle *h) { return h ? h->launches : -1; }
+
+}  // extern "C"

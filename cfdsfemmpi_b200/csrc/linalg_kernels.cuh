@@ -1,0 +1,479 @@
+// Sparse and dense linear-algebra kernels for the nodal-block (BSR) system:
+// SpMV with the preconditioner fused into its epilogue, deterministic
+// reductions, and the device-side pieces of restarted GMRES (PETSc 3.10
+// KSPGMRES semantics: classical Gram-Schmidt, left preconditioning,
+// preconditioned-residual norm, KSPConvergedDefault; the reference calls it
+// from src/base/SolverPetsc.cpp:253).
+//
+// Determinism: every reduction uses a fixed grid (RED_BLOCKS CTAs), a fixed
+// per-thread stride, a fixed in-CTA tree, and a last-CTA pass that adds the
+// per-CTA partials in index order, so results do not depend on scheduling.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cfdgpu {
+
+constexpr int RED_BLOCKS = 296;     // 2 x 148 SMs
+constexpr int RED_THREADS = 256;
+constexpr int MDOT_CHUNK = 8;       // basis vectors per CTA row in the multi-dot
+
+// ---------------------------------------------------------------------------
+// GMRES control block (device memory).  One thread (the last CTA of a
+// reduction kernel) updates it; every other kernel only reads it.
+struct GmresState {
+  int it;          // Arnoldi columns built in the current cycle
+  int its;         // total iterations (KSP iteration count)
+  int reason;      // KSPConvergedReason, 0 while iterating
+  int active;      // current cycle continues
+  int m;           // restart length
+  int maxit;
+  double rtol, atol, dtol;
+  double rnorm0, ttol;
+  double res;      // current residual-norm estimate
+  double tt;       // norm of the newest Krylov vector
+  double v0scale;  // 1/res for V_0 (0: leave V_0 as is)
+  unsigned int counter;
+};
+
+struct GmresArrays {
+  double *H;       // (m+1) x m, row-major H[r*m + c]
+  double *cs, *sn; // m
+  double *grs;     // m+1
+  double *y;       // m
+  double *partial; // scratch for reductions: (m+1) * RED_BLOCKS doubles
+};
+
+__device__ __forceinline__ int ksp_converged(GmresState *s, int n_its, double rnorm)
+{
+  if (n_its == 0) {
+    s->rnorm0 = rnorm;
+    s->ttol = fmax(s->rtol * rnorm, s->atol);
+  }
+  if (isnan(rnorm) || isinf(rnorm)) return -9;            // KSP_DIVERGED_NANORINF
+  if (rnorm <= s->ttol) return (rnorm < s->atol) ? 3 : 2; // KSP_CONVERGED_ATOL / RTOL
+  if (rnorm >= s->dtol * s->rnorm0) return -4;            // KSP_DIVERGED_DTOL
+  return 0;
+}
+
+// Block-level sum (fixed tree); result valid in thread 0.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NT / 32; k++) r += sh[k];
+  }
+  __syncthreads();
+  return r;
+}
+
+// Returns true in exactly one CTA (the last to arrive), after all CTAs'
+// partials are visible.
+__device__ __forceinline__ bool last_block(unsigned int *counter, unsigned int nblocks)
+{
+  __shared__ bool amlast;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(counter, 1u);
+    amlast = (t == nblocks - 1);
+  }
+  __syncthreads();
+  if (amlast) {
+    __threadfence();
+    if (threadIdx.x == 0) *counter = 0u;
+  }
+  return amlast;
+}
+
+// ---------------------------------------------------------------------------
+// BSR SpMV, 4x4 FP64 blocks: one warp per block row; each lane loads 16 B of
+// a block (row q/2, columns 2(q%2), 2(q%2)+1 of block 'sub') so a warp
+// instruction reads four consecutive 128-B blocks.  MODE 0: y = M^-1 (A x),
+// MODE 1: y = M^-1 (b - A x).  PC: 0 none, 1 jacobi (dinv), 2 point-block
+// (binv, 4x4 per node, row-major).
+template <int MODE, int PC>
+__global__ void __launch_bounds__(256)
+bsr4_spmv_f64(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
+              const double *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
+              const double *__restrict__ dinv, const double *__restrict__ binv, double *__restrict__ y,
+              const GmresState *__restrict__ st, int j)
+{
+  if (st && (!st->active || st->it != j)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nrows) return;
+  const int sub = lane >> 3, q = lane & 7, row = q >> 1, cp = (q & 1) * 2;
+  const int kb0 = rowptr[warp], kb1 = rowptr[warp + 1];
+  double acc = 0.0;
+  for (int kb = kb0 + sub; kb < kb1; kb += 4) {
+    const int c = colidx[kb];
+    const double2 a = *reinterpret_cast<const double2 *>(val + (int64_t)kb * 16 + row * 4 + cp);
+    const double2 xv = *reinterpret_cast<const double2 *>(x + (int64_t)c * 4 + cp);
+    acc = fma(a.x, xv.x, acc);
+    acc = fma(a.y, xv.y, acc);
+  }
+  acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+  // lanes 0,2,4,6 hold rows 0..3
+  const int64_t r = (int64_t)warp * 4 + row;
+  double v = acc;
+  if (MODE == 1) v = b[r] - acc;
+  if (PC == 2) {
+    const double v0 = __shfl_sync(0xffffffffu, v, 0), v1 = __shfl_sync(0xffffffffu, v, 2);
+    const double v2 = __shfl_sync(0xffffffffu, v, 4), v3 = __shfl_sync(0xffffffffu, v, 6);
+    if (lane < 8 && (lane & 1) == 0) {
+      const double *Bi = binv + (int64_t)warp * 16 + row * 4;
+      y[r] = Bi[0] * v0 + Bi[1] * v1 + Bi[2] * v2 + Bi[3] * v3;
+    }
+  } else if (lane < 8 && (lane & 1) == 0) {
+    y[r] = (PC == 1) ? dinv[r] * v : v;
+  }
+}
+
+// Generic BSR SpMV for any block size NB (used for 3x3 blocks): one thread
+// per scalar row.
+template <int NB, int MODE, int PC, typename VT>
+__global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
+                                 const VT *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
+                                 const double *__restrict__ dinv, const double *__restrict__ binv,
+                                 double *__restrict__ y, const GmresState *__restrict__ st, int j)
+{
+  if (st && (!st->active || st->it != j)) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t node = t / NB;
+  const int row = (int)(t % NB);
+  if (node >= nrows) return;
+  double acc = 0.0;
+  for (int kb = rowptr[node]; kb < rowptr[node + 1]; kb++) {
+    const int c = colidx[kb];
+    const VT *a = val + (int64_t)kb * NB * NB + row * NB;
+#pragma unroll
+    for (int q = 0; q < NB; q++) acc = fma((double)a[q], x[(int64_t)c * NB + q], acc);
+  }
+  double v = (MODE == 1) ? b[t] - acc : acc;
+  if (PC == 1) v *= dinv[t];
+  if (PC == 2) {
+    // point block needs the whole node: recompute the node's other rows
+    double vv[NB];
+#pragma unroll
+    for (int rr = 0; rr < NB; rr++) {
+      double s = 0.0;
+      for (int kb = rowptr[node]; kb < rowptr[node + 1]; kb++) {
+        const int c = colidx[kb];
+        const VT *a = val + (int64_t)kb * NB * NB + rr * NB;
+#pragma unroll
+        for (int q = 0; q < NB; q++) s = fma((double)a[q], x[(int64_t)c * NB + q], s);
+      }
+      vv[rr] = (MODE == 1) ? b[node * NB + rr] - s : s;
+    }
+    double z = 0.0;
+#pragma unroll
+    for (int q = 0; q < NB; q++) z += binv[node * NB * NB + row * NB + q] * vv[q];
+    v = z;
+  }
+  y[t] = v;
+}
+
+// z = M^-1 r (stand-alone preconditioner application)
+template <int NB>
+__global__ void pc_apply(int64_t n, int pc, const double *__restrict__ dinv, const double *__restrict__ binv,
+                         const double *__restrict__ r, double *__restrict__ z)
+{
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  if (pc == 2) {
+    const int64_t node = t / NB;
+    const int row = (int)(t % NB);
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < NB; q++) s += binv[node * NB * NB + row * NB + q] * r[node * NB + q];
+    z[t] = s;
+  } else if (pc == 1) {
+    z[t] = dinv[t] * r[t];
+  } else {
+    z[t] = r[t];
+  }
+}
+
+// Scalar-diagonal inverse and point-block inverses of the assembled matrix.
+template <int NB, typename VT>
+__global__ void build_jacobi(int nnode, const int32_t *__restrict__ diag_slot, const VT *__restrict__ val,
+                             double *__restrict__ dinv, double *__restrict__ binv, int pc)
+{
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= nnode) return;
+  const VT *B = val + (int64_t)diag_slot[node] * NB * NB;
+  if (pc == 1) {
+#pragma unroll
+    for (int a = 0; a < NB; a++) {
+      const double d = (double)B[a * NB + a];
+      dinv[(int64_t)node * NB + a] = (d != 0.0) ? 1.0 / d : 1.0;
+    }
+    return;
+  }
+  // Gauss-Jordan with partial pivoting on the NB x NB diagonal block
+  double A[NB][NB], I[NB][NB];
+#pragma unroll
+  for (int a = 0; a < NB; a++)
+#pragma unroll
+    for (int c = 0; c < NB; c++) { A[a][c] = (double)B[a * NB + c]; I[a][c] = (a == c) ? 1.0 : 0.0; }
+#pragma unroll
+  for (int c = 0; c < NB; c++) {
+    int piv = c;
+#pragma unroll
+    for (int r = c + 1; r < NB; r++)
+      if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      if (piv != c) {
+        double t = A[c][k]; A[c][k] = A[piv][k]; A[piv][k] = t;
+        t = I[c][k]; I[c][k] = I[piv][k]; I[piv][k] = t;
+      }
+    }
+    const double p = A[c][c];
+    const double d = (p != 0.0) ? 1.0 / p : 1.0;
+#pragma unroll
+    for (int k = 0; k < NB; k++) { A[c][k] *= d; I[c][k] *= d; }
+#pragma unroll
+    for (int r = 0; r < NB; r++) {
+      if (r == c) continue;
+      const double f = A[r][c];
+#pragma unroll
+      for (int k = 0; k < NB; k++) { A[r][k] -= f * A[c][k]; I[r][k] -= f * I[c][k]; }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NB; a++)
+#pragma unroll
+    for (int c = 0; c < NB; c++) binv[(int64_t)node * NB * NB + a * NB + c] = I[a][c];
+}
+
+// ---------------------------------------------------------------------------
+// deterministic 2-norm: out[0] = ||x||; partials in scratch
+__global__ void __launch_bounds__(RED_THREADS)
+norm2_kernel(int64_t n, const double *__restrict__ x, double *__restrict__ partial, unsigned int *counter,
+             double *__restrict__ out)
+{
+  __shared__ double sh[RED_THREADS / 32];
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS)
+    s = fma(x[i], x[i], s);
+  s = block_sum<RED_THREADS>(s, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (last_block(counter, gridDim.x)) {
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (unsigned int k = 0; k < gridDim.x; k++) t += partial[k];
+      out[0] = sqrt(t);
+    }
+  }
+}
+
+// GMRES cycle start: res = ||V0||, convergence test at its, v0scale.
+__global__ void __launch_bounds__(RED_THREADS)
+gmres_start(int64_t n, const double *__restrict__ v0, GmresState *st, GmresArrays ga)
+{
+  __shared__ double sh[RED_THREADS / 32];
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS)
+    s = fma(v0[i], v0[i], s);
+  s = block_sum<RED_THREADS>(s, sh);
+  if (threadIdx.x == 0) ga.partial[blockIdx.x] = s;
+  if (last_block(&st->counter, gridDim.x)) {
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (unsigned int k = 0; k < gridDim.x; k++) t += ga.partial[k];
+      const double res = sqrt(t);
+      st->res = res;
+      st->it = 0;
+      ga.grs[0] = res;
+      st->v0scale = (res != 0.0) ? 1.0 / res : 0.0;
+      if (res == 0.0) {
+        if (st->its == 0) { st->rnorm0 = 0.0; st->ttol = st->atol; }
+        st->reason = 3;   // KSP_CONVERGED_ATOL: zero residual on entry
+        st->active = 0;
+      } else {
+        st->reason = ksp_converged(st, st->its, res);
+        st->active = (st->reason == 0 && st->its < st->maxit && st->m > 0) ? 1 : 0;
+      }
+    }
+  }
+}
+
+__global__ void scale_v0(int64_t n, double *__restrict__ v0, const GmresState *__restrict__ st)
+{
+  const double s = st->v0scale;
+  if (s == 0.0) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v0[i] *= s;
+}
+
+// h_k = <w, V_k>, k = 0..j (classical Gram-Schmidt dot products).
+// grid: (RED_BLOCKS, ceil((j+1)/MDOT_CHUNK)).  The last CTA writes H[k][j].
+__global__ void __launch_bounds__(RED_THREADS)
+gmres_mdot(int64_t n, const double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
+{
+  if (!st->active || st->it != j) return;
+  __shared__ double sh[RED_THREADS / 32];
+  const int k0 = blockIdx.y * MDOT_CHUNK;
+  const int nk = min(MDOT_CHUNK, j + 1 - k0);
+  const double *w = V + (int64_t)(j + 1) * ldv;
+  double s[MDOT_CHUNK];
+#pragma unroll
+  for (int q = 0; q < MDOT_CHUNK; q++) s[q] = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
+    const double wi = w[i];
+#pragma unroll
+    for (int q = 0; q < MDOT_CHUNK; q++)
+      if (q < nk) s[q] = fma(wi, V[(int64_t)(k0 + q) * ldv + i], s[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < MDOT_CHUNK; q++) {
+    if (q < nk) {
+      const double t = block_sum<RED_THREADS>(s[q], sh);
+      if (threadIdx.x == 0) ga.partial[(int64_t)(k0 + q) * gridDim.x + blockIdx.x] = t;
+    }
+  }
+  if (last_block(&st->counter, gridDim.x * gridDim.y)) {
+    const int m = st->m;
+    for (int k = threadIdx.x; k <= j; k += blockDim.x) {
+      double t = 0.0;
+      for (unsigned int b = 0; b < gridDim.x; b++) t += ga.partial[(int64_t)k * gridDim.x + b];
+      ga.H[(int64_t)k * m + j] = t;
+    }
+  }
+}
+
+// w -= sum_k H[k][j] V_k, then ||w||, Hessenberg/Givens update and the
+// convergence test (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
+__global__ void __launch_bounds__(RED_THREADS)
+gmres_maxpy_norm(int64_t n, double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
+{
+  if (!st->active || st->it != j) return;
+  __shared__ double sh[RED_THREADS / 32];
+  __shared__ double hk[1024];
+  const int m = st->m;
+  for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[(int64_t)k * m + j];
+  __syncthreads();
+  double *w = V + (int64_t)(j + 1) * ldv;
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
+    double wi = w[i];
+    for (int k = 0; k <= j; k++) wi = fma(-hk[k], V[(int64_t)k * ldv + i], wi);
+    w[i] = wi;
+    s = fma(wi, wi, s);
+  }
+  s = block_sum<RED_THREADS>(s, sh);
+  if (threadIdx.x == 0) ga.partial[blockIdx.x] = s;
+  if (last_block(&st->counter, gridDim.x)) {
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (unsigned int b = 0; b < gridDim.x; b++) t += ga.partial[b];
+      const double tt = sqrt(t);
+      st->tt = tt;
+      double *H = ga.H;
+      const int it = j;
+      H[(int64_t)(it + 1) * m + it] = tt;
+      double hapbnd = fabs(tt / ga.grs[it]);
+      if (hapbnd > 1.0e-30) hapbnd = 1.0e-30;
+      const bool hapend = tt < hapbnd;
+      for (int q = 1; q <= it; q++) {
+        const double a = H[(int64_t)(q - 1) * m + it];
+        const double bq = H[(int64_t)q * m + it];
+        H[(int64_t)(q - 1) * m + it] = ga.cs[q - 1] * a + ga.sn[q - 1] * bq;
+        H[(int64_t)q * m + it] = ga.cs[q - 1] * bq - ga.sn[q - 1] * a;
+      }
+      double res;
+      int reason = 0;
+      if (!hapend) {
+        const double a = H[(int64_t)it * m + it], bq = H[(int64_t)(it + 1) * m + it];
+        const double r = sqrt(a * a + bq * bq);
+        if (r == 0.0) {
+          reason = -2;   // KSP_DIVERGED_NULL
+          res = st->res;
+        } else {
+          ga.cs[it] = a / r;
+          ga.sn[it] = bq / r;
+          ga.grs[it + 1] = -(ga.sn[it] * ga.grs[it]);
+          ga.grs[it] = ga.cs[it] * ga.grs[it];
+          H[(int64_t)it * m + it] = ga.cs[it] * a + ga.sn[it] * bq;
+          res = fabs(ga.grs[it + 1]);
+        }
+      } else {
+        res = 0.0;
+      }
+      if (reason == 0) {
+        st->it = it + 1;
+        st->its = st->its + 1;
+        st->res = res;
+        reason = ksp_converged(st, st->its, res);
+        if (hapend && reason == 0) reason = -5;   // KSP_DIVERGED_BREAKDOWN
+      }
+      st->reason = reason;
+      st->active = (reason == 0 && st->it < m && st->its < st->maxit) ? 1 : 0;
+    }
+  }
+}
+
+// V_{j+1} /= tt (VecNormalize), only if step j ran
+__global__ void gmres_scale_next(int64_t n, double *__restrict__ V, int64_t ldv, int j, const GmresState *__restrict__ st)
+{
+  if (st->it != j + 1) return;
+  const double tt = st->tt;
+  if (tt == 0.0) return;
+  const double s = 1.0 / tt;
+  double *w = V + (int64_t)(j + 1) * ldv;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    w[i] *= s;
+}
+
+// KSPGMRESBuildSoln: back substitution for the it x it triangular system.
+__global__ void gmres_backsub(GmresState *st, GmresArrays ga)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int last = st->it - 1;
+  const int m = st->m;
+  if (last < 0) return;
+  const double *H = ga.H;
+  double *y = ga.y;
+  y[last] = (H[(int64_t)last * m + last] != 0.0) ? ga.grs[last] / H[(int64_t)last * m + last] : 0.0;
+  for (int ii = 1; ii <= last; ii++) {
+    const int k = last - ii;
+    double t = ga.grs[k];
+    for (int q = k + 1; q <= last; q++) t = t - H[(int64_t)k * m + q] * y[q];
+    y[k] = (H[(int64_t)k * m + k] != 0.0) ? t / H[(int64_t)k * m + k] : 0.0;
+  }
+}
+
+// x += sum_{k < it} y_k V_k
+__global__ void gmres_update_x(int64_t n, double *__restrict__ x, const double *__restrict__ V, int64_t ldv,
+                               const GmresState *__restrict__ st, GmresArrays ga)
+{
+  const int it = st->it;
+  if (it <= 0) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < it; k++) s = fma(ga.y[k], V[(int64_t)k * ldv + i], s);
+    x[i] += s;
+  }
+}
+
+__global__ void gmres_init(GmresState *st, int m, int maxit, double rtol, double atol, double dtol)
+{
+  if (threadIdx.x || blockIdx.x) return;
+  st->it = 0; st->its = 0; st->reason = 0; st->active = 0;
+  st->m = m; st->maxit = maxit; st->rtol = rtol; st->atol = atol; st->dtol = dtol;
+  st->rnorm0 = 0.0; st->ttol = 0.0; st->res = 0.0; st->tt = 0.0; st->v0scale = 0.0;
+  st->counter = 0u;
+}
+
+}  // namespace cfdgpu

@@ -1,0 +1,139 @@
+// Host-side set-up of the nodal-block matrix structure; see setup.h.
+#include "setup.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <numeric>
+
+namespace cfdgpu {
+
+std::string build_topology(int nNode, int nElem, int npe, int ndof, const int32_t *conn, int nDBC,
+                           const int32_t *dbc_node, const int32_t *dbc_dof, const double *dbc_value,
+                           Topology &t)
+{
+  t = Topology();
+  t.nNode = nNode; t.nElem = nElem; t.npe = npe; t.ndof = ndof;
+  if (nNode <= 0 || nElem <= 0) return "empty mesh";
+  for (int64_t k = 0; k < (int64_t)nElem * npe; k++)
+    if (conn[k] < 0 || conn[k] >= nNode) return "connectivity refers to a node outside [0, nNode)";
+
+  // node -> incident elements
+  std::vector<int32_t> eptr(nNode + 1, 0);
+  for (int64_t k = 0; k < (int64_t)nElem * npe; k++) eptr[conn[k] + 1]++;
+  for (int n = 0; n < nNode; n++) eptr[n + 1] += eptr[n];
+  std::vector<int32_t> elist(eptr[nNode]);
+  {
+    std::vector<int32_t> fill(nNode, 0);
+    for (int e = 0; e < nElem; e++)
+      for (int a = 0; a < npe; a++) {
+        int n = conn[(int64_t)e * npe + a];
+        elist[eptr[n] + fill[n]++] = e;
+      }
+  }
+
+  // node graph (block sparsity), sorted per row
+  t.rowptr.assign(nNode + 1, 0);
+  {
+    std::vector<int32_t> mark(nNode, -1);
+    for (int n = 0; n < nNode; n++) {
+      int cnt = 0;
+      for (int k = eptr[n]; k < eptr[n + 1]; k++) {
+        const int32_t *c = conn + (int64_t)elist[k] * npe;
+        for (int a = 0; a < npe; a++)
+          if (mark[c[a]] != n) { mark[c[a]] = n; cnt++; }
+      }
+      t.rowptr[n + 1] = t.rowptr[n] + cnt;
+    }
+    t.colidx.resize(t.rowptr[nNode]);
+    std::fill(mark.begin(), mark.end(), -1);
+    for (int n = 0; n < nNode; n++) {
+      int pos = t.rowptr[n];
+      for (int k = eptr[n]; k < eptr[n + 1]; k++) {
+        const int32_t *c = conn + (int64_t)elist[k] * npe;
+        for (int a = 0; a < npe; a++)
+          if (mark[c[a]] != n) { mark[c[a]] = n; t.colidx[pos++] = c[a]; }
+      }
+      std::sort(t.colidx.begin() + t.rowptr[n], t.colidx.begin() + t.rowptr[n + 1]);
+    }
+  }
+
+  // slot map
+  t.slot.resize((int64_t)nElem * npe * npe);
+  for (int e = 0; e < nElem; e++) {
+    const int32_t *c = conn + (int64_t)e * npe;
+    for (int i = 0; i < npe; i++) {
+      const int32_t *b = t.colidx.data() + t.rowptr[c[i]];
+      const int32_t *en = t.colidx.data() + t.rowptr[c[i] + 1];
+      for (int j = 0; j < npe; j++) {
+        const int32_t *p = std::lower_bound(b, en, c[j]);
+        t.slot[((int64_t)e * npe + i) * npe + j] = (int32_t)(p - t.colidx.data());
+      }
+    }
+  }
+
+  // greedy colouring in element order
+  t.color.assign(nElem, -1);
+  t.ncolors = 0;
+  for (int e = 0; e < nElem; e++) {
+    uint64_t used = 0;
+    const int32_t *c = conn + (int64_t)e * npe;
+    for (int a = 0; a < npe; a++)
+      for (int k = eptr[c[a]]; k < eptr[c[a] + 1]; k++) {
+        int cc = t.color[elist[k]];
+        if (cc >= 0 && cc < 64) used |= (1ULL << cc);
+      }
+    int cc = 0;
+    while (cc < 64 && (used & (1ULL << cc))) cc++;
+    if (cc >= 64) return "element colouring needs more than 64 colours";
+    t.color[e] = cc;
+    t.ncolors = std::max(t.ncolors, cc + 1);
+  }
+  t.color_ptr.assign(t.ncolors + 1, 0);
+  for (int e = 0; e < nElem; e++) t.color_ptr[t.color[e] + 1]++;
+  for (int c = 0; c < t.ncolors; c++) t.color_ptr[c + 1] += t.color_ptr[c];
+  t.color_elems.resize(nElem);
+  {
+    std::vector<int32_t> fill(t.ncolors, 0);
+    for (int e = 0; e < nElem; e++) t.color_elems[t.color_ptr[t.color[e]] + fill[t.color[e]]++] = e;
+  }
+
+  // first writer of each block, in launch order (colour, then element id)
+  {
+    std::vector<uint8_t> seen(t.colidx.size(), 0);
+    for (int k = 0; k < nElem; k++) {
+      int e = t.color_elems[k];
+      for (int p = 0; p < npe * npe; p++) {
+        int32_t &s = t.slot[(int64_t)e * npe * npe + p];
+        if (!seen[s]) { seen[s] = 1; s = -s - 1; }
+      }
+    }
+  }
+
+  // Dirichlet sets and free-dof numbering
+  t.fixmask.assign(nNode, 0);
+  t.dbc_index.resize(nDBC);
+  t.dbc_value.resize(nDBC);
+  std::vector<int32_t> mult((int64_t)nNode * ndof, 0);
+  for (int k = 0; k < nDBC; k++) {
+    if (dbc_node[k] < 0 || dbc_node[k] >= nNode || dbc_dof[k] < 0 || dbc_dof[k] >= ndof)
+      return "Dirichlet entry outside the mesh";
+    int32_t g = dbc_node[k] * ndof + dbc_dof[k];
+    t.dbc_index[k] = g;
+    t.dbc_value[k] = dbc_value[k];
+    t.fixmask[dbc_node[k]] |= (uint8_t)(1u << dbc_dof[k]);
+    mult[g]++;
+  }
+  t.dofmap.assign((int64_t)nNode * ndof, -1);
+  t.nfree = 0;
+  for (int64_t g = 0; g < (int64_t)nNode * ndof; g++) {
+    if (mult[g]) {
+      t.fixed_dofs.push_back((int32_t)g);
+      t.dbc_mult.push_back(mult[g]);
+    } else {
+      t.dofmap[g] = t.nfree++;
+    }
+  }
+  return "";
+}
+
+}  // namespace cfdgpu

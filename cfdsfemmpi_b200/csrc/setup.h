@@ -1,0 +1,49 @@
+// Host-side set-up of the nodal-block matrix structure (no CUDA).
+//
+// Builds, deterministically from the mesh alone:
+//   * the node graph (nodes sharing an element), sorted per node: the block
+//     sparsity of the BSR matrix.  With Dirichlet rows/columns deleted, its
+//     scalar expansion equals the free-dof pattern the reference inserts into
+//     PETSc (src/base/StabFEM2.cpp:192-227);
+//   * the element -> block slot map: for element e and local nodes (i, j) the
+//     index of block (conn[e][i], conn[e][j]); the first writer of every block
+//     in colour order is marked by storing -slot-1;
+//   * a greedy element colouring (elements that share a node differ), visited
+//     in element-id order;
+//   * the free-dof numbering of the reference (node-major, skipping
+//     prescribed (node, dof) pairs, StabFEM2.cpp:57-81) and the Dirichlet sets.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cfdgpu {
+
+struct Topology {
+  int nNode = 0, nElem = 0, npe = 0, ndof = 0;
+  std::vector<int32_t> rowptr;       // nNode+1
+  std::vector<int32_t> colidx;       // nnzb
+  std::vector<int32_t> slot;         // nElem*npe*npe
+  std::vector<int32_t> color;        // nElem
+  std::vector<int32_t> color_ptr;    // ncolors+1
+  std::vector<int32_t> color_elems;  // nElem, grouped by colour, ascending id inside a colour
+  int ncolors = 0;
+  std::vector<int32_t> dofmap;       // nNode*ndof -> free index or -1
+  int nfree = 0;
+  std::vector<int32_t> fixed_dofs;   // sorted distinct prescribed dofs
+  // Dirichlet list in input order (node*ndof+dof, value)
+  std::vector<int32_t> dbc_index;
+  std::vector<double> dbc_value;
+  // per distinct prescribed dof: how many list entries name it (the reference
+  // adds solnApplied once per entry, StabFEM2.cpp:719-730)
+  std::vector<int32_t> dbc_mult;
+  std::vector<uint8_t> fixmask;      // per node: bit d set when dof d is prescribed
+  int64_t nnzb() const { return (int64_t)colidx.size(); }
+};
+
+// Returns "" on success, else an error message.
+std::string build_topology(int nNode, int nElem, int npe, int ndof, const int32_t *conn, int nDBC,
+                           const int32_t *dbc_node, const int32_t *dbc_dof, const double *dbc_value,
+                           Topology &t);
+
+}  // namespace cfdgpu

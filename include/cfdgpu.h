@@ -1,0 +1,199 @@
+/*
+ * cfdgpu.h -- C ABI of the B200 (sm_100a) time-step library for stabilised
+ * linear-element incompressible Navier-Stokes (quad4/tri3/hex8/tet4).
+ *
+ * The library replaces, behind plain pointers and sizes, the per-time-step
+ * body of the cfdsfemmpi solver:
+ *   - the element loop + PETSc assembly of StabFEM::solveFullyImplicit
+ *     (src/base/StabFEM2.cpp:654-740) and the element virtual
+ *     ElementBase::calcStiffnessAndResidual (src/base/ElementBase.h:87),
+ *   - the SolverPetsc object (src/base/SolverPetsc.h:15-64: initialise,
+ *     zeroMtx, assembleMatrixAndVectorSerial, factoriseAndSolve),
+ *   - SolutionData's per-step vector algebra (src/base/SolutionData.cpp:64-91).
+ * The caller keeps the reference's driver (time loop, ramp, output) and calls
+ * cfdgpu_step once per time step.
+ *
+ * Conventions: every function returns 0 on success or a negative CFDGPU_E*
+ * code; cfdgpu_last_error(h) describes the last failure on a handle.  No
+ * function calls exit().  One handle per host thread; a handle owns one CUDA
+ * stream and all of its device memory.  Full nodal vectors use the
+ * reference's layout: index node*ndof + dof, ndof = ndim + 1 (u, v[, w], p).
+ */
+#ifndef CFDGPU_H
+#define CFDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define CFDGPU_OK 0
+#define CFDGPU_EINVAL (-1)      /* bad argument or wrong state (SolverPetsc.cpp:205-209) */
+#define CFDGPU_ECUDA (-2)       /* CUDA runtime error */
+#define CFDGPU_ENEGJAC (-3)     /* negative Jacobian (reference exits, e.g. Hexa8Node.cpp:79-84) */
+#define CFDGPU_EKSP (-4)        /* linear solve diverged (reference exits, SolverPetsc.cpp:264-269) */
+#define CFDGPU_ENOMEM (-5)
+#define CFDGPU_ENODEV (-6)      /* no CUDA device / kernels not loadable */
+
+/* element types, as selected in StabFEM::prepareInputData (StabFEM.cpp:351-366) */
+#define CFDGPU_TRI3 0
+#define CFDGPU_QUAD4 1
+#define CFDGPU_TET4 2
+#define CFDGPU_HEX8 3
+
+/* preconditioners (PETSc -pc_type names) */
+#define CFDGPU_PC_NONE 0
+#define CFDGPU_PC_JACOBI 1      /* inverse of the scalar diagonal */
+#define CFDGPU_PC_PBJACOBI 2    /* inverse of each node's ndof x ndof diagonal block */
+
+/* precision modes */
+#define CFDGPU_PREC_FP64 0      /* FP64 element kernels, matrix and Krylov solve */
+#define CFDGPU_PREC_MIXED 1     /* FP32 tangent + FP32 inner GMRES, FP64 residual/refinement */
+
+/* Mesh: borrowed host arrays, copied at create (StabFEM::readInputData,
+ * StabFEM.cpp:80-264).  conn is 0-based, nElem*npElem; DBC entries are
+ * 0-based (node, dof, value) triples. */
+typedef struct cfdgpu_mesh {
+  int ndim;
+  int npElem;
+  int nNode;
+  int nElem;
+  const double *coords;     /* nNode*ndim */
+  const int32_t *conn;      /* nElem*npElem */
+  int nDBC;
+  const int32_t *dbc_node;
+  const int32_t *dbc_dof;
+  const double *dbc_value;
+} cfdgpu_mesh;
+
+/* Control parameters (StabFEM::readControlParameters, StabFEM.cpp:268-322)
+ * plus the Newton settings the reference hard-codes (StabFEM2.cpp:654,749). */
+typedef struct cfdgpu_control {
+  double rho, mu;
+  double bodyforce[3];      /* read but unused by the active elements */
+  double stab[3];           /* SUPG, PSPG, LSIC factors (elemData[8..10]) */
+  int tis;
+  double rhoInf;
+  double dt;
+  double newton_tol;        /* absolute residual 2-norm, reference: 1e-8 */
+  int newton_max_iter;      /* reference: 10 */
+} cfdgpu_control;
+
+/* Krylov options (PETSc option semantics: -ksp_gmres_restart, -ksp_rtol,
+ * -ksp_atol, -ksp_divtol, -ksp_max_it, -pc_type). */
+typedef struct cfdgpu_solver_opts {
+  int restart;
+  double rtol, atol, dtol;
+  int max_it;
+  int pc_type;
+  int precision;            /* CFDGPU_PREC_* */
+  int inner_restart;        /* mixed mode: FP32 inner GMRES restart (0: = restart) */
+  double inner_rtol;        /* mixed mode: inner relative tolerance per refinement pass */
+  int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
+} cfdgpu_solver_opts;
+
+#define CFDGPU_MAX_NEWTON 32
+
+typedef struct cfdgpu_step_stats {
+  int newton_iters;                     /* assemblies done (including the converged check) */
+  int converged;                        /* residual < newton_tol within the cap */
+  double norms[CFDGPU_MAX_NEWTON];      /* residual 2-norm per Newton iteration */
+  int ksp_its[CFDGPU_MAX_NEWTON];       /* Krylov iterations per solve */
+  int ksp_reason[CFDGPU_MAX_NEWTON];    /* PETSc-style KSPConvergedReason per solve */
+  int refinements[CFDGPU_MAX_NEWTON];   /* mixed mode: outer refinement passes per solve */
+  double ms_assembly, ms_solver, ms_total;
+} cfdgpu_step_stats;
+
+typedef struct cfdgpu_handle cfdgpu_handle;
+
+/* Replaces StabFEM::setSolver/prepareMatrixPattern (StabFEM2.cpp:10-319) and
+ * SolverPetsc::initialise (SolverPetsc.cpp:30-116): copies the mesh, builds
+ * the nodal-block (BSR) pattern, element colouring and element->block slot
+ * map, Dirichlet sets, and allocates all device state (zero initial state,
+ * SolutionData::initialise, SolutionData.cpp:16-35). */
+int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfdgpu_solver_opts *opts,
+                  cfdgpu_handle **out);
+int cfdgpu_destroy(cfdgpu_handle *h);
+const char *cfdgpu_last_error(const cfdgpu_handle *h);
+
+/* Replaces the body of the time loop of StabFEM::solveFullyImplicit
+ * (StabFEM2.cpp:632-799): setTimeParam + timeUpdate, assignBoundaryConditions
+ * with the caller's ramp factor, then the Newton loop (assembly, residual
+ * norm, GMRES solve, update).  Returns CFDGPU_EKSP when a linear solve
+ * diverges (the reference exits there); Newton non-convergence is reported
+ * in stats->converged and is not an error (the reference continues). */
+int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_stats *stats);
+
+/* Full nodal vector soln (SolutionData::soln), host memory, nNode*ndof. */
+int cfdgpu_get_solution(cfdgpu_handle *h, double *soln);
+int cfdgpu_set_solution(cfdgpu_handle *h, const double *soln);
+/* Device pointer of the handle's soln vector (for callers that keep data on
+ * the GPU) and the handle's CUDA stream (cudaStream_t). */
+int cfdgpu_device_solution(cfdgpu_handle *h, double **dptr);
+int cfdgpu_stream(cfdgpu_handle *h, void **stream);
+/* Overwrite the time-history vectors (solnPrev, solnDotPrev) from host
+ * memory; NULL leaves one unchanged. */
+int cfdgpu_set_history(cfdgpu_handle *h, const double *solnPrev, const double *solnDot);
+
+/* Element routine parity hook (ElementBase::calcStiffnessAndResidual): for
+ * the listed elements, K_e (nsize x nsize, row-major, local index
+ * node*ndof+dof) and F_e from the handle's current solnPrev, solnCur and
+ * solnDotCur under time scheme tis/rhoInf/dt, without lifting or Dirichlet
+ * masking.  nsize = npElem*ndof.  K and F are host arrays. */
+int cfdgpu_element_matrices(cfdgpu_handle *h, const int32_t *elem_ids, int n, double *K, double *F);
+/* Set solnPrev, solnCur, solnDotCur directly (host arrays, nNode*ndof) and
+ * the td[] vector used by element kernels (time scheme tis). */
+int cfdgpu_set_element_state(cfdgpu_handle *h, const double *solnPrev, const double *solnCur,
+                             const double *solnDotCur);
+
+/* Sizes of the structures exported by cfdgpu_export_pattern. */
+typedef struct cfdgpu_pattern_info {
+  int nNode, nElem, npElem, ndof;
+  int64_t nnzb;             /* BSR blocks */
+  int ncolors;
+  int nfixed;               /* distinct Dirichlet dofs */
+  int nfree;                /* free dofs (reference ntotdofs_global) */
+} cfdgpu_pattern_info;
+int cfdgpu_pattern_info_get(cfdgpu_handle *h, cfdgpu_pattern_info *info);
+/* rowptr (nNode+1), colidx (nnzb), slot (nElem*npElem*npElem; entries < 0
+ * mark the first writer of a block: block = -slot-1), color (nElem),
+ * color_ptr (ncolors+1), color_elems (nElem), fixed_dofs (nfixed, sorted),
+ * dofmap (nNode*ndof: free index or -1, StabFEM2.cpp:57-81).  Any pointer
+ * may be NULL. */
+int cfdgpu_export_pattern(cfdgpu_handle *h, int32_t *rowptr, int32_t *colidx, int32_t *slot, int32_t *color,
+                          int32_t *color_ptr, int32_t *color_elems, int32_t *fixed_dofs, int32_t *dofmap);
+
+/* Host-only variant (no device, no handle): builds the same structures from
+ * a mesh.  Call once with NULL arrays to get the sizes in *info, then with
+ * arrays of those sizes. */
+int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int32_t *rowptr, int32_t *colidx,
+                         int32_t *slot, int32_t *color, int32_t *color_ptr, int32_t *color_elems,
+                         int32_t *fixed_dofs, int32_t *dofmap);
+
+/* Assemble (iteration-0 semantics when iter == 0: lifting included) at the
+ * current state and copy the BSR values (nnzb*ndof*ndof, FP64, block
+ * row-major) and the RHS (nNode*ndof) to host.  Uses the td[] of the last
+ * step or of cfdgpu_set_element_state. */
+int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double *rhs);
+
+/* Solve A x = b on the handle's last assembled matrix with the handle's
+ * GMRES options; b and x are host arrays (nNode*ndof, zero at Dirichlet
+ * dofs).  its/reason may be NULL. */
+int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, int *reason);
+
+/* Timers in the reference's categories (StabFEM::printComputerTimes,
+ * StabFEM.cpp:711-727), seconds: [0] pattern, [1] assembly, [2] solver,
+ * [3] post-process (unused by the library), [4] total in cfdgpu_step. */
+int cfdgpu_timers(cfdgpu_handle *h, double t[5]);
+
+/* Number of kernel launches issued by this handle so far. */
+int64_t cfdgpu_launch_count(cfdgpu_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFDGPU_H */

@@ -1,0 +1,151 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every symbol include/cfdgpu.h declares, and the host-built structures
+(free-dof numbering, block pattern, Dirichlet sets, colouring, slot map)
+match the oracle bit for bit."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from cfdsfemmpi_b200 import _lib, io, meshgen, pattern_build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "cfdgpu.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*\*?\s*(cfdgpu_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(L, s), s
+    assert sorted(_lib.EXPORTS) == syms
+
+
+def _meshes(golden_dir):
+    yield "ldc2d10", meshgen.cavity2d(10)
+    yield "ldc2d_graded", meshgen.cavity2d(7, pin_node=3, graded_beta=1.2)
+    yield "ldc3d6", meshgen.cavity3d(6)
+    yield "golden10", io.read_mesh(os.path.join(golden_dir, "ldc2dquad10", "LDC2Dquad10"))
+    # unstructured-numbered golden mesh (16,641 nodes)
+    yield "mesh2", io.read_mesh(os.path.join(golden_dir, "ldc2dquad-mesh2", "LDC2Dquad-mesh2"))
+    # tri3 and tet4: split the structured meshes
+    q = meshgen.cavity2d(5)
+    tri = q.conn[:, [0, 1, 2]].tolist() + q.conn[:, [0, 2, 3]].tolist()
+    yield "tri", io.Mesh(ndim=2, npElem=3, coords=q.coords, conn=np.array(tri, np.int32), dbc=q.dbc,
+                         output_nodes=np.zeros(0, np.int32))
+    h = meshgen.cavity3d(3)
+    tets = []
+    for c in h.conn:
+        for t in ([0, 1, 3, 4], [1, 2, 3, 6], [1, 3, 4, 6], [1, 4, 5, 6], [3, 4, 6, 7]):
+            tets.append(c[t])
+    yield "tet", io.Mesh(ndim=3, npElem=4, coords=h.coords, conn=np.array(tets, np.int32), dbc=h.dbc,
+                         output_nodes=np.zeros(0, np.int32))
+
+
+def scalar_pattern_from_blocks(d, ndof):
+    """Expand the BSR block pattern to the free-dof scalar pattern."""
+    rowptr, colidx, dofmap = d["rowptr"], d["colidx"], d["dofmap"]
+    nfree = int(d["info"].nfree)
+    rp = [0]
+    ci = []
+    for n in range(len(rowptr) - 1):
+        cols = colidx[rowptr[n]:rowptr[n + 1]]
+        for a in range(ndof):
+            if dofmap[n * ndof + a] < 0:
+                continue
+            for mm in cols:
+                for b in range(ndof):
+                    c = dofmap[mm * ndof + b]
+                    if c >= 0:
+                        ci.append(c)
+            rp.append(len(ci))
+    assert len(rp) == nfree + 1
+    return np.array(rp, np.int32), np.array(ci, np.int32)
+
+
+def test_pattern_and_sets_match_oracle(golden_dir):
+    L = oracle.lib()
+    for name, mesh in _meshes(golden_dir):
+        d = pattern_build(mesh)
+        ref = oracle.OracleFEM(mesh, io.Control(), solver="lu")
+        # free-dof numbering and Dirichlet set (StabFEM2.cpp:57-81)
+        assert np.array_equal(d["dofmap"], ref.dofmap), name
+        assert np.array_equal(d["fixed_dofs"], np.unique(ref.dbc_index).astype(np.int32)), name
+        assert d["info"].nfree == ref.ntot
+        # scalar pattern with Dirichlet rows/columns deleted == reference pattern
+        if mesh.nNode < 5000:
+            rp, ci = scalar_pattern_from_blocks(d, mesh.ndof)
+            assert np.array_equal(rp, ref.rowptr), name
+            assert np.array_equal(ci, ref.colidx), name
+        # colouring: same greedy rule as the oracle
+        col = np.zeros(mesh.nElem, np.int32)
+        nc = L.orc_color(mesh.nNode, mesh.nElem, mesh.npElem, np.ascontiguousarray(mesh.conn, np.int32), col)
+        assert nc == d["info"].ncolors and np.array_equal(col, d["color"]), name
+
+
+def test_colouring_and_slot_map_invariants(golden_dir):
+    for name, mesh in _meshes(golden_dir):
+        d = pattern_build(mesh)
+        npe = mesh.npElem
+        conn = mesh.conn
+        color = d["color"]
+        # no two elements of one colour share a node
+        for c in range(d["info"].ncolors):
+            els = np.nonzero(color == c)[0]
+            nodes = conn[els].ravel()
+            assert len(np.unique(nodes)) == len(nodes), (name, c)
+        # colour-ordered element list
+        ce, cp = d["color_elems"], d["color_ptr"]
+        for c in range(d["info"].ncolors):
+            seg = ce[cp[c]:cp[c + 1]]
+            assert np.all(color[seg] == c) and np.all(np.diff(seg) > 0)
+        # slot map points at block (conn[e][i], conn[e][j])
+        slot = d["slot"].reshape(mesh.nElem, npe, npe)
+        first = slot < 0
+        s = np.where(first, -slot - 1, slot)
+        rowptr, colidx = d["rowptr"], d["colidx"]
+        assert np.array_equal(colidx[s], np.broadcast_to(conn[:, None, :], s.shape))
+        row_of = np.repeat(np.arange(mesh.nNode), np.diff(rowptr))
+        assert np.array_equal(row_of[s], np.broadcast_to(conn[:, :, None], s.shape))
+        # every block has exactly one first writer, the earliest in launch order
+        nnzb = int(d["info"].nnzb)
+        assert np.bincount(s[first], minlength=nnzb).max() == 1
+        assert np.bincount(s[first], minlength=nnzb).min() == 1
+        order = np.empty(mesh.nElem, np.int64)
+        order[ce] = np.arange(mesh.nElem)
+        pos = np.broadcast_to(order[:, None, None], s.shape)
+        earliest = np.full(nnzb, np.iinfo(np.int64).max)
+        np.minimum.at(earliest, s.ravel(), pos.ravel())
+        assert np.array_equal(earliest[s[first]], pos[first])
+
+
+def test_pattern_sizes_3d32():
+    """Sizes quoted for the 32^3 graded cube: 35,937 nodes, 912,673 blocks,
+    18,439 prescribed dofs (walls x 3 + one pressure pin), 8 colours."""
+    d = pattern_build(meshgen.cavity3d(32))
+    pi = d["info"]
+    assert (pi.nNode, pi.nElem, pi.nnzb, pi.nfixed, pi.ncolors) == (35937, 32768, 912673, 18439, 8)
+    assert pi.nfree == 35937 * 4 - 18439
+
+
+def test_create_fails_loudly_without_device():
+    """No CPU fallback: without a GPU, cfdgpu_create returns an error."""
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("GPU present")
+    m, c, _ = meshgen.CASES["ldc2d_10"]()
+    with pytest.raises(_lib.CfdGpuError) as ei:
+        _lib.Handle(m, c)
+    assert ei.value.code in (_lib.ENODEV, _lib.ECUDA)

@@ -1,0 +1,243 @@
+"""GPU parity: the CUDA library, called through its C ABI, against the CPU
+oracle on the same inputs.
+
+Tolerances (FP64 path):
+  * element matrices: normwise relative 1e-13 (max|dK| / max|K|);
+  * assembled free-dof matrix and residual: normwise relative 1e-13;
+  * fields after N steps with the same solver options: relative L2 1e-8;
+  * shipped known-answer tests: the reference's own check (1e-4 per node),
+    and 1e-7 max difference to the shipped values.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from cfdsfemmpi_b200 import Handle, StabFEM, io, meshgen
+
+pytestmark = pytest.mark.gpu
+
+
+def _distorted(mesh, amp, seed):
+    rng = np.random.default_rng(seed)
+    m = io.Mesh(ndim=mesh.ndim, npElem=mesh.npElem, coords=mesh.coords.copy(), conn=mesh.conn, dbc=mesh.dbc,
+                output_nodes=mesh.output_nodes)
+    h = 1.0 / 40
+    m.coords += amp * h * rng.uniform(-1, 1, m.coords.shape)
+    return m
+
+
+def _tri_tet(kind):
+    if kind == "tri":
+        q = meshgen.cavity2d(6)
+        tri = q.conn[:, [0, 1, 2]].tolist() + q.conn[:, [0, 2, 3]].tolist()
+        return io.Mesh(ndim=2, npElem=3, coords=q.coords, conn=np.array(tri, np.int32), dbc=q.dbc,
+                       output_nodes=np.zeros(0, np.int32))
+    h = meshgen.cavity3d(3)
+    tets = []
+    for c in h.conn:
+        for t in ([0, 1, 3, 4], [1, 2, 3, 6], [1, 3, 4, 6], [1, 4, 5, 6], [3, 4, 6, 7]):
+            tets.append(c[t])
+    return io.Mesh(ndim=3, npElem=4, coords=h.coords, conn=np.array(tets, np.int32), dbc=h.dbc,
+                   output_nodes=np.zeros(0, np.int32))
+
+
+MESHES = {
+    "quad4": lambda: _distorted(meshgen.cavity2d(8), 0.3, 1),
+    "hex8": lambda: _distorted(meshgen.cavity3d(4), 0.1, 2),
+    "tri3": lambda: _tri_tet("tri"),
+    "tet4": lambda: _tri_tet("tet"),
+}
+
+
+def _random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    return [rng.uniform(-1, 1, n) for _ in range(3)]
+
+
+@pytest.mark.parametrize("kind", list(MESHES))
+@pytest.mark.parametrize("tis", [0, 2])
+def test_element_matrices_match_oracle(kind, tis):
+    mesh = MESHES[kind]()
+    ctrl = meshgen.control_for(5, 0.1, 0.01, tis=tis)
+    h = Handle(mesh, ctrl)
+    prev, cur, dot = _random_state(mesh.nNode * mesh.ndof, 11)
+    h.set_element_state(prev, cur, dot)
+    ids = np.arange(mesh.nElem, dtype=np.int32)
+    K, F = h.element_matrices(ids)
+    td = oracle.time_params(tis, ctrl.rhoInf, ctrl.dt)
+    ed = ctrl.elem_data()
+    ndof = mesh.ndof
+    worstK = worstF = 0.0
+    for e in range(mesh.nElem):
+        nodes = mesh.conn[e]
+        g = (nodes[:, None] * ndof + np.arange(ndof)).ravel()
+        Kr, Fr, _, rc = oracle.element(mesh.elem_type, mesh.coords[nodes], prev[g], cur[g], dot[g], ed, td)
+        worstK = max(worstK, np.abs(K[e] - Kr).max() / np.abs(Kr).max())
+        worstF = max(worstF, np.abs(F[e] - Fr).max() / np.abs(Fr).max())
+    h.close()
+    assert worstK < 1e-13, worstK
+    assert worstF < 1e-13, worstF
+
+
+def _free_matrix(h, vals, rhs, mesh):
+    """Expand the GPU BSR to the reference's free-dof CSR (dense for small cases)."""
+    d = h.export_pattern()
+    ndof = mesh.ndof
+    dofmap = d["dofmap"]
+    nfree = d["info"].nfree
+    A = np.zeros((nfree, nfree))
+    rowptr, colidx = d["rowptr"], d["colidx"]
+    for n in range(mesh.nNode):
+        for k in range(rowptr[n], rowptr[n + 1]):
+            m = colidx[k]
+            for a in range(ndof):
+                r = dofmap[n * ndof + a]
+                if r < 0:
+                    continue
+                for b in range(ndof):
+                    c = dofmap[m * ndof + b]
+                    if c >= 0:
+                        A[r, c] = vals[k, a, b]
+    b = rhs[dofmap >= 0]
+    return A, b, d
+
+
+@pytest.mark.parametrize("kind", list(MESHES))
+def test_assembly_matches_oracle(kind):
+    """Assembly without lifting (Newton iterations >= 1) from a random state;
+    the lifting path is covered by the full time-step tests."""
+    mesh = MESHES[kind]()
+    ctrl = meshgen.control_for(5, 0.1, 0.01, tis=2)
+    ref = oracle.OracleFEM(mesh, ctrl, solver="lu")
+    ref.td = oracle.time_params(ctrl.tis, ctrl.rhoInf, ctrl.dt)
+    rng = np.random.default_rng(5)
+    ref.soln = rng.uniform(-0.5, 0.5, ref.soln.shape)
+    ref.solnDot = rng.uniform(-0.5, 0.5, ref.soln.shape)
+    ref.time_update()
+    ref.solnApplied[ref.dbc_index] = ref.dbc_value * 0.3 - ref.soln[ref.dbc_index]
+    ref.update_iter_step()
+    h = Handle(mesh, ctrl)
+    h.set_element_state(ref.solnPrev, ref.solnCur, ref.solnDotCur)
+    vals, rhs = h.assemble_export(1)
+    A, b, d = _free_matrix(h, vals, rhs, mesh)
+    ref.assemble(1)
+    A_ref = ref.csr().toarray()
+    assert np.abs(A - A_ref).max() / np.abs(A_ref).max() < 1e-13
+    assert np.abs(b - ref.rhs).max() / np.abs(ref.rhs).max() < 1e-13
+    # Dirichlet rows/columns are identity inside the blocks
+    fixed = d["fixed_dofs"]
+    ndof = mesh.ndof
+    rowptr, colidx = d["rowptr"], d["colidx"]
+    for g in fixed[:50]:
+        n, a = divmod(int(g), ndof)
+        for k in range(rowptr[n], rowptr[n + 1]):
+            row = vals[k, a, :]
+            if colidx[k] == n:
+                assert row[a] == 1.0 and np.count_nonzero(row) == 1
+            else:
+                assert np.count_nonzero(row) == 0
+    h.close()
+
+
+def test_assembly_is_deterministic():
+    mesh = MESHES["hex8"]()
+    ctrl = meshgen.control_for(5, 0.1, 0.001)
+    prev, cur, dot = _random_state(mesh.nNode * mesh.ndof, 3)
+    out = []
+    for _ in range(2):
+        h = Handle(mesh, ctrl)
+        h.set_element_state(prev, cur, dot)
+        out.append(h.assemble_export(0))
+        out.append(h.assemble_export(0))
+        h.close()
+    for v, r in out[1:]:
+        assert np.array_equal(v, out[0][0]) and np.array_equal(r, out[0][1])
+
+
+def _run_gpu(mesh, ctrl, steps=None, **kw):
+    h = Handle(mesh, ctrl, **kw)
+    timeNow = ctrl.dt
+    stats = []
+    n = ctrl.stepsMax if steps is None else steps
+    for _ in range(n):
+        tf = timeNow if timeNow <= 1.0 else 1.0
+        stats.append(h.step(timeNow, tf).as_dict())
+        timeNow = timeNow + ctrl.dt
+        if timeNow > ctrl.timeFinal:
+            break
+    s = h.get_solution()
+    h.close()
+    return s, stats
+
+
+def test_ldc2d_gmres_jacobi_matches_oracle():
+    """2D cavity, gen-alpha rho_inf=0, dt 0.1, 20 steps, GMRES(50)+Jacobi rtol 1e-10."""
+    mesh, ctrl, _ = meshgen.CASES["ldc2d_10"]()
+    ref = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=50, rtol=1e-10, pc="jacobi")
+    ref.solve()
+    s, stats = _run_gpu(mesh, ctrl, restart=50, rtol=1e-10, pc="jacobi")
+    rel = np.linalg.norm(s - ref.soln) / np.linalg.norm(ref.soln)
+    assert rel < 1e-8, rel
+    assert len(stats) == 20 and all(st["converged"] for st in stats)
+    # Krylov iteration counts follow the oracle's PETSc-semantics GMRES
+    its_gpu = [st["ksp_its"][0] for st in stats]
+    its_ref = [st["gmres_its"][0] for st in ref.stats]
+    assert max(abs(a - b) for a, b in zip(its_gpu, its_ref)) <= 2, (its_gpu, its_ref)
+
+
+def test_ldc3d_small_matches_oracle():
+    mesh, ctrl, _ = meshgen.case_hex(6, 3)
+    ref = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=200, rtol=1e-10, pc="jacobi", threads=4)
+    ref.solve()
+    s, stats = _run_gpu(mesh, ctrl, restart=200, rtol=1e-10, pc="jacobi")
+    rel = np.linalg.norm(s - ref.soln) / np.linalg.norm(ref.soln)
+    assert rel < 1e-8, rel
+    its_gpu = [st["ksp_its"] for st in stats]
+    its_ref = [st["gmres_its"] for st in ref.stats]
+    assert its_gpu and all(len(a) == len(b) for a, b in zip(its_gpu, its_ref))
+
+
+def test_ldc3d_pbjacobi_matches_lu():
+    mesh, ctrl, _ = meshgen.case_hex(5, 2)
+    ref = oracle.OracleFEM(mesh, ctrl, solver="lu")
+    ref.solve()
+    s, stats = _run_gpu(mesh, ctrl, restart=200, rtol=1e-12, pc="pbjacobi")
+    rel = np.linalg.norm(s - ref.soln) / np.linalg.norm(ref.soln)
+    assert rel < 1e-8, rel
+
+
+def test_kat_ldc2dquad10_through_driver(golden_dir, tmp_path):
+    d = os.path.join(golden_dir, "ldc2dquad10")
+    fem = StabFEM()
+    fem.readInputData(os.path.join(d, "LDC2Dquad10"))
+    fem.readControlParameters(os.path.join(d, "control-parameters-ldc-Re100.dat"))
+    fem.prepareInputData()
+    fem.write_forces = False
+    fem.setSolver(1, None, False, options=os.path.join(d, "petsc_options.dat"))
+    assert fem.solveFullyImplicit() == 0
+    ref = os.path.join(d, "test-ldc-stru-nelem10-ref.dat")
+    assert fem.checkResult(ref) == 0
+    diff = np.abs(io.read_result(ref) - fem.solution().reshape(-1, 3)).max()
+    assert diff < 1e-7
+    out = tmp_path / "res.dat"
+    fem.writeResult(str(out))
+    assert io.check_result(str(out), fem.solution(), 121, 2) == 0
+    fem.deallocatePetscObjects()
+
+
+@pytest.mark.slow
+def test_kat_ldc2dquad_mesh2_through_driver(golden_dir):
+    d = os.path.join(golden_dir, "ldc2dquad-mesh2")
+    fem = StabFEM()
+    fem.readInputData(os.path.join(d, "LDC2Dquad-mesh2"))
+    fem.readControlParameters(os.path.join(d, "control-parameters-Re1000.dat"))
+    fem.write_forces = False
+    fem.setSolver(1, None, False, options=os.path.join(d, "petsc_options.dat"))
+    assert fem.solveFullyImplicit() == 0
+    ref = os.path.join(d, "test-ldc-stru-mesh2-ref.dat")
+    assert fem.checkResult(ref) == 0
+    diff = np.abs(io.read_result(ref) - fem.solution().reshape(-1, 3)).max()
+    assert diff < 1e-6
+    fem.deallocatePetscObjects()
