@@ -1,0 +1,345 @@
+"""Benchmark: time steps/s of the 3D lid-driven-cavity hex8 solve on B200.
+
+One "step" is one time step of the solver (time update, boundary conditions,
+Newton loop with assembly and GMRES solves to the absolute 1e-8 residual).
+The default workload is the graded 32^3 hex8 cavity (32,768 elements, 35,937
+nodes, Re = 1000, dt = 0.1, generalised-alpha rho_inf = 0) with GMRES(400) and
+point-block Jacobi at rtol 1e-10.  W warm-up steps from rest run first, then
+exactly K timed steps.
+
+Arms:
+  default          the CUDA library through its C ABI (device-resident state);
+                   also an end-to-end number through the same API with the
+                   state crossing host<->device every step.
+  --impl reference the CPU restatement of the reference path (oracle/) on all
+                   host cores, same workload, same solver options.
+
+Multi-GPU (torchrun, N > 1): the path does not shard, every rank advances an
+independent replica ("replicas only"); value = N*K / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D LDC hex8 time steps/s on 1 B200 (surrogate-guess vs plain) at 1e-8 residual"
+
+WORKLOADS = {
+    # name: (n per side, steps in the configuration, solver options)
+    "ldc3d_32": (32, 50, {"restart": 400, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 10000}),
+    "ldc3d_16": (16, 50, {"restart": 400, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 10000}),
+    "ldc3d_64": (64, 20, {"restart": 800, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 20000}),
+    "ldc3d_115": (115, 20, {"restart": 1000, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 40000}),
+}
+
+SMI_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="ldc3d_32", choices=list(WORKLOADS))
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def make_case(name):
+    from cfdsfemmpi_b200 import meshgen
+    n, steps, opts = WORKLOADS[name]
+    mesh, ctrl, _ = meshgen.case_hex(n, steps, mu=0.001, dt=0.1)
+    return mesh, ctrl, dict(opts)
+
+
+def workload_config(name, mesh, opts, extra=None):
+    n = WORKLOADS[name][0]
+    cfg = {"workload": f"{name}: graded-cube lid-driven cavity, {n}^3 hex8 ({mesh.nElem} elements, "
+                       f"{mesh.nNode} nodes, {mesh.nNode * 4} dofs), Re 1000, dt 0.1, gen-alpha rho_inf 0",
+           "method": "plain (reference-identical constant predictor), FP64",
+           "solver": f"Newton to 1e-8 abs; GMRES({opts['restart']}) + {opts['pc']}, rtol {opts['rtol']:g}",
+           "l2": "flushed between timed steps (256 MiB write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={SMI_QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier_max(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.barrier()
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from cfdsfemmpi_b200 import Handle
+
+    torch.cuda.set_device(local)
+    mesh, ctrl, opts = make_case(args.workload)
+    h = Handle(mesh, ctrl, **opts)
+    stream = torch.cuda.ExternalStream(h.stream_ptr())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    timeNow = ctrl.dt
+    stats = []
+
+    def one_step(record):
+        nonlocal timeNow
+        tf = timeNow if timeNow <= 1.0 else 1.0
+        st = h.step(timeNow, tf).as_dict()
+        timeNow = timeNow + ctrl.dt
+        if record:
+            stats.append(st)
+        return st
+
+    for _ in range(args.warmup):
+        one_step(False)
+    torch.cuda.synchronize()
+    launches0 = h.launch_count()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one_step(True)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = h.launch_count() - launches0
+    t_max = barrier_max(world, total_ms)
+    value = world * args.steps / (t_max * 1e-3)
+
+    # dominant kernel: profile one more step with per-launch CUDA events
+    h.set_profiling(True)
+    one_step(False)
+    kinds = {k: h.kernel_stats(k) for k in ("spmv", "ortho", "elem_k", "elem_f")}
+    h.set_profiling(False)
+    prof_total = sum(v[1] for v in kinds.values())
+    dom = max(kinds, key=lambda k: kinds[k][1])
+    nl, ms, by = kinds[dom]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = (by / nl) / (ms / nl * 1e-3) / 1e9 if nl else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload, {}).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_src,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "algorithmic_bytes_per_launch": by / nl if nl else None,
+                "avg_launch_ms": ms / nl if nl else None, "launches_profiled": nl,
+                "share_of_profiled_step": ms / prof_total if prof_total else None,
+                "kernels": {k: {"launches": v[0], "ms": round(v[1], 4),
+                                "gbs": (v[2] / (v[1] * 1e-3) / 1e9) if v[1] else None} for k, v in kinds.items()}}
+
+    # end to end through the C ABI with host buffers: H2D of the state from
+    # pinned memory, the step, D2H of the result, every step
+    e2e = None
+    if not args.no_e2e:
+        n = h.n
+        pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        h.get_solution_ptr(pin.data_ptr())
+        e2e_steps = max(1, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            h.set_solution_ptr(pin.data_ptr())
+            one_step(False)
+            h.get_solution_ptr(pin.data_ptr())
+        dt_e2e = time.perf_counter() - t0
+        dt_e2e = barrier_max(world, dt_e2e)
+        e2e = {"value": world * e2e_steps / dt_e2e, "unit": "steps/s", "steps": e2e_steps,
+               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+               "api": "cfdgpu_set_solution + cfdgpu_step + cfdgpu_get_solution (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(h, mesh, ctrl, opts, timeNow)
+    h.close()
+    its = [sum(s["ksp_its"]) for s in stats]
+    newt = [s["newton_iters"] for s in stats]
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: graded-cube hex8 cavity generated in-process (no dataset)",
+            "config": workload_config(args.workload, mesh, opts,
+                                      {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                       "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps} of the run"}),
+            "newton_iters_per_step": statistics.mean(newt) if newt else None,
+            "gmres_iters_per_step": statistics.mean(its) if its else None,
+            "gmres_iters": its,
+            "all_converged": all(s["converged"] for s in stats),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks}
+    return line
+
+
+def cpu_baseline_sample(h, mesh, ctrl, opts, timeNow):
+    """Time one time step of the same run on the host cores with the CPU
+    restatement, starting from the GPU run's current state."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    threads = os.cpu_count() or 1
+    fem = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=opts["restart"], rtol=opts["rtol"],
+                           pc=opts["pc"], max_it=opts["max_it"], threads=threads)
+    fem.soln = h.get_solution()
+    _, fem.solnDot = h.get_history()
+    fem.timeNow = timeNow
+    t0 = time.perf_counter()
+    st = fem.step()
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"one full time step (t = {timeNow:.1f}) of the same run from the GPU state; "
+                      f"{sum(st['gmres_its'])} GMRES its, {dt:.1f} s"}
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference path, all host threads."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    mesh, ctrl, opts = make_case(args.workload)
+    threads = os.cpu_count() or 1
+    fem = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=opts["restart"], rtol=opts["rtol"], pc=opts["pc"],
+                           max_it=opts["max_it"], threads=threads)
+
+    def one():
+        fem.step()
+        fem.timeNow = fem.timeNow + ctrl.dt
+
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    dt = time.perf_counter() - t0
+    stats = fem.stats[args.warmup:]
+    value = args.steps / dt
+    return {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic: graded-cube hex8 cavity generated in-process (no dataset)",
+            "config": workload_config(args.workload, mesh, opts, {"parallelism": "host cores"}),
+            "gmres_iters_per_step": statistics.mean(sum(s["gmres_its"]) for s in stats),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": f"time steps {args.warmup + 1}..{args.warmup + args.steps} of the run, "
+                                       "C restatement (OpenMP) of the reference path"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # host-only arm: rank 0 runs it, other ranks have nothing to do
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), rank)
+        if line is not None:
+            print(json.dumps(line))
+        return
+    world, rank, local = dist_setup(args)
+    line = run_ours(args, world, rank, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

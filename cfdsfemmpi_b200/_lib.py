@@ -17,10 +17,12 @@ LIB_PATH = os.path.join(HERE, "libcfdgpu.so")
 # the symbols declared in include/cfdgpu.h, in declaration order
 EXPORTS = [
     "cfdgpu_create", "cfdgpu_destroy", "cfdgpu_last_error", "cfdgpu_step", "cfdgpu_get_solution",
-    "cfdgpu_set_solution", "cfdgpu_device_solution", "cfdgpu_stream", "cfdgpu_set_history",
+    "cfdgpu_set_solution", "cfdgpu_device_solution", "cfdgpu_stream", "cfdgpu_set_history", "cfdgpu_get_history",
     "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
     "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
+    "cfdgpu_set_profiling", "cfdgpu_kernel_stats",
 ]
+KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
 
 OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV = 0, -1, -2, -3, -4, -5, -6
 PC = {"none": 0, "jacobi": 1, "pbjacobi": 2}
@@ -93,6 +95,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_device_solution.argtypes = [vp, ctypes.POINTER(vp)]
     L.cfdgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.cfdgpu_set_history.argtypes = [vp, vp, vp]
+    L.cfdgpu_get_history.argtypes = [vp, vp, vp]
     L.cfdgpu_element_matrices.argtypes = [vp, vp, ip, vp, vp]
     L.cfdgpu_set_element_state.argtypes = [vp, vp, vp, vp]
     L.cfdgpu_pattern_info_get.argtypes = [vp, ctypes.POINTER(PatternInfo)]
@@ -103,6 +106,9 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_timers.argtypes = [vp, vp]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
+    L.cfdgpu_set_profiling.argtypes = [vp, ip]
+    L.cfdgpu_kernel_stats.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:
         if name not in ("cfdgpu_last_error", "cfdgpu_launch_count"):
             getattr(L, name).restype = ctypes.c_int
@@ -225,6 +231,18 @@ class Handle:
         b = None if solnDot is None else np.ascontiguousarray(solnDot, dtype=np.float64)
         self._check(self._L.cfdgpu_set_history(self.h, _ptr(a), _ptr(b)))
 
+    def get_history(self):
+        a, b = np.empty(self.n), np.empty(self.n)
+        self._check(self._L.cfdgpu_get_history(self.h, _ptr(a), _ptr(b)))
+        return a, b
+
+    def set_solution_ptr(self, host_ptr: int):
+        """H2D copy of soln from a raw host pointer (e.g. pinned memory)."""
+        self._check(self._L.cfdgpu_set_solution(self.h, host_ptr))
+
+    def get_solution_ptr(self, host_ptr: int):
+        self._check(self._L.cfdgpu_get_solution(self.h, host_ptr))
+
     def stream_ptr(self) -> int:
         p = ctypes.c_void_p()
         self._check(self._L.cfdgpu_stream(self.h, ctypes.byref(p)))
@@ -282,3 +300,16 @@ class Handle:
 
     def launch_count(self) -> int:
         return int(self._L.cfdgpu_launch_count(self.h))
+
+    def set_profiling(self, on: bool):
+        self._check(self._L.cfdgpu_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_stats(self, kind: str):
+        """(launches, total device ms, total algorithmic bytes) for a kernel kind
+        since profiling was switched on."""
+        n = ctypes.c_int64()
+        ms = ctypes.c_double()
+        by = ctypes.c_double()
+        self._check(self._L.cfdgpu_kernel_stats(self.h, KIND[kind], ctypes.byref(n), ctypes.byref(ms),
+                                                ctypes.byref(by)))
+        return int(n.value), float(ms.value), float(by.value)

@@ -73,7 +73,50 @@ struct cfdgpu_handle {
   GmresState *h_gst = nullptr;       // pinned
   bool assembled_K = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-kernel event timing
+  bool prof = false;
+  std::vector<cudaEvent_t> pev;          // pool of 2*PROF_POOL events
+  std::vector<int> pkind;                // kind of each recorded pair
+  std::vector<double> pbytes;            // algorithmic bytes of each recorded launch
+  int pused = 0;
+  int64_t prof_launches[CFDGPU_KIND_COUNT] = {0, 0, 0, 0};
+  double prof_ms[CFDGPU_KIND_COUNT] = {0, 0, 0, 0};
+  double prof_bytes[CFDGPU_KIND_COUNT] = {0, 0, 0, 0};
 };
+
+static const int PROF_POOL = 32768;
+
+// flush recorded event pairs into the per-kind totals
+static void prof_collect(cfdgpu_handle *h)
+{
+  if (!h->pused) return;
+  cudaEventSynchronize(h->pev[2 * (h->pused - 1) + 1]);
+  for (int i = 0; i < h->pused; i++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->pev[2 * i], h->pev[2 * i + 1]) == cudaSuccess) {
+      h->prof_ms[h->pkind[i]] += ms;
+      h->prof_launches[h->pkind[i]] += 1;
+      h->prof_bytes[h->pkind[i]] += h->pbytes[i];
+    }
+  }
+  h->pused = 0;
+}
+
+static int prof_begin(cfdgpu_handle *h, int kind, double bytes)
+{
+  if (!h->prof) return -1;
+  if (h->pused >= PROF_POOL) prof_collect(h);
+  const int i = h->pused++;
+  h->pkind[i] = kind;
+  h->pbytes[i] = bytes;
+  cudaEventRecord(h->pev[2 * i], h->stream);
+  return i;
+}
+
+static void prof_end(cfdgpu_handle *h, int i)
+{
+  if (i >= 0) cudaEventRecord(h->pev[2 * i + 1], h->stream);
+}
 
 #define CK(call)                                                                   \
   do {                                                                             \
@@ -242,12 +285,20 @@ static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, doub
   constexpr int GROUPS = (GS == 32) ? 4 : 8;
   const int grid = (nel + GROUPS - 1) / GROUPS;
   if (grid <= 0) return 0;
+  // algorithmic bytes of one assembly (BSR written once, RHS, coordinates,
+  // connectivity, three state vectors), shared evenly by the colour launches
+  const double Vb = 8.0 * h->n;
+  const double asm_bytes = ((MODE == MODE_RESIDUAL) ? 0.0 : 8.0 * h->topo.nnzb() * h->ndof * h->ndof) + Vb +
+                           8.0 * h->nNode * h->ndim + 4.0 * h->nElem * h->npe + 3.0 * Vb;
+  const int pi = prof_begin(h, MODE == MODE_RESIDUAL ? CFDGPU_KIND_ELEM_F : CFDGPU_KIND_ELEM_K,
+                            asm_bytes / std::max(1, h->topo.ncolors));
   ElemParams P;
   P.rho = h->ctrl.rho; P.mu = h->ctrl.mu; P.af = h->td[2]; P.am = h->td[1]; P.acceFact = h->td[8];
   P.stab0 = h->ctrl.stab[0]; P.stab1 = h->ctrl.stab[1]; P.stab2 = h->ctrl.stab[2];
   element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
       elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
       h->rhs, outK, outF, h->negjac);
+  prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "element_kernel");
 }
@@ -308,6 +359,12 @@ static int build_pc(cfdgpu_handle *h)
 static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y, const GmresState *st, int j)
 {
   const int pc = h->opts.pc_type;
+  // algorithmic bytes: blocks + column indices + row pointers + x + y (+ b)
+  // + the preconditioner's data
+  const double V = 8.0 * h->n, B = (double)h->topo.nnzb(), bb = (double)h->ndof * h->ndof;
+  const double pcb = (pc == 1) ? V : (pc == 2) ? 8.0 * bb * h->nNode : 0.0;
+  const int pi = prof_begin(h, CFDGPU_KIND_SPMV, B * bb * 8.0 + 4.0 * B + 4.0 * (h->nNode + 1) + 2.0 * V +
+                                                     (mode == 1 ? V : 0.0) + pcb);
   if (h->ndof == 4) {
     const int grid = (int)((h->nNode * 32LL + 255) / 256);
 #define SPMV4(MO, PCV)                                                                                  \
@@ -331,6 +388,7 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
     }
 #undef SPMV3
   }
+  prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "bsr_spmv");
 }
@@ -378,8 +436,11 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
       for (int j = j0; j < std::min(m, j0 + CH); j++) {
         if ((rc = spmv_pc(h, 0, V + (int64_t)j * ldv, nullptr, V + (int64_t)(j + 1) * ldv, st, j))) return rc;
         dim3 g2(RED_BLOCKS, (j + 1 + MDOT_CHUNK - 1) / MDOT_CHUNK);
+        // multi-dot reads V_0..V_j and w; update reads them again and writes w
+        const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 5.0) * 8.0 * n);
         gmres_mdot<<<g2, RED_THREADS, 0, h->stream>>>(n, V, ldv, j, st, h->ga);
         gmres_maxpy_norm<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, ldv, j, st, h->ga);
+        prof_end(h, pi);
         gmres_scale_next<<<vgrid, 256, 0, h->stream>>>(n, V, ldv, j, st);
         h->launches += 3;
       }
@@ -540,6 +601,7 @@ int cfdgpu_destroy(cfdgpu_handle *h)
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_scalar) cudaFreeHost(h->h_scalar);
   if (h->h_gst) cudaFreeHost(h->h_gst);
+  for (auto &e : h->pev) cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -649,6 +711,15 @@ int cfdgpu_set_history(cfdgpu_handle *h, const double *solnPrev, const double *s
   if (!h) return CFDGPU_EINVAL;
   if (solnPrev) CK(cudaMemcpyAsync(h->prev, solnPrev, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
   if (solnDot) CK(cudaMemcpyAsync(h->dot, solnDot, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int cfdgpu_get_history(cfdgpu_handle *h, double *solnPrev, double *solnDot)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (solnPrev) CK(cudaMemcpyAsync(solnPrev, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  if (solnDot) CK(cudaMemcpyAsync(solnDot, h->dot, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return 0;
 }
@@ -765,5 +836,31 @@ int cfdgpu_timers(cfdgpu_handle *h, double t[5])
 }
 
 int64_t cfdgpu_launch_count(cfdgpu_handle *h) { return h ? h->launches : -1; }
+
+int cfdgpu_set_profiling(cfdgpu_handle *h, int on)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (on && h->pev.empty()) {
+    h->pev.resize(2 * PROF_POOL);
+    h->pkind.resize(PROF_POOL);
+    h->pbytes.resize(PROF_POOL);
+    for (auto &e : h->pev) CK(cudaEventCreate(&e));
+  }
+  if (!on) prof_collect(h);
+  h->prof = on != 0;
+  for (int k = 0; k < CFDGPU_KIND_COUNT; k++) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; h->prof_bytes[k] = 0.0; }
+  return 0;
+}
+
+int cfdgpu_kernel_stats(cfdgpu_handle *h, int kind, int64_t *launches, double *total_ms, double *total_bytes)
+{
+  if (!h || kind < 0 || kind >= CFDGPU_KIND_COUNT) return CFDGPU_EINVAL;
+  CK(cudaStreamSynchronize(h->stream));
+  prof_collect(h);
+  if (launches) *launches = h->prof_launches[kind];
+  if (total_ms) *total_ms = h->prof_ms[kind];
+  if (total_bytes) *total_bytes = h->prof_bytes[kind];
+  return 0;
+}
 
 }  // extern "C"

@@ -134,9 +134,12 @@ int cfdgpu_set_solution(cfdgpu_handle *h, const double *soln);
  * the GPU) and the handle's CUDA stream (cudaStream_t). */
 int cfdgpu_device_solution(cfdgpu_handle *h, double **dptr);
 int cfdgpu_stream(cfdgpu_handle *h, void **stream);
-/* Overwrite the time-history vectors (solnPrev, solnDotPrev) from host
- * memory; NULL leaves one unchanged. */
+/* Overwrite the time-history vectors (solnPrev, solnDot) from host memory;
+ * NULL leaves one unchanged.  solnDot becomes solnDotPrev at the next step
+ * (SolutionData::timeUpdate, SolutionData.cpp:64-78). */
 int cfdgpu_set_history(cfdgpu_handle *h, const double *solnPrev, const double *solnDot);
+/* Copy solnPrev and solnDot to host memory (NULL skips one). */
+int cfdgpu_get_history(cfdgpu_handle *h, double *solnPrev, double *solnDot);
 
 /* Element routine parity hook (ElementBase::calcStiffnessAndResidual): for
  * the listed elements, K_e (nsize x nsize, row-major, local index
@@ -191,6 +194,18 @@ int cfdgpu_timers(cfdgpu_handle *h, double t[5]);
 
 /* Number of kernel launches issued by this handle so far. */
 int64_t cfdgpu_launch_count(cfdgpu_handle *h);
+
+/* Per-kernel device timing with CUDA events on the handle's stream (off by
+ * default).  Kinds: */
+#define CFDGPU_KIND_SPMV 0        /* BSR SpMV with the fused preconditioner (Krylov operator) */
+#define CFDGPU_KIND_ELEM_K 1      /* element kernel, tangent + residual, one launch per colour */
+#define CFDGPU_KIND_ELEM_F 2      /* element kernel, residual only */
+#define CFDGPU_KIND_ORTHO 3       /* Gram-Schmidt multi-dot + update/norm pair */
+#define CFDGPU_KIND_COUNT 4
+int cfdgpu_set_profiling(cfdgpu_handle *h, int on);
+/* Totals since profiling was switched on: launches, summed device ms, and
+ * summed algorithmic bytes (the minimum DRAM traffic of each launch). */
+int cfdgpu_kernel_stats(cfdgpu_handle *h, int kind, int64_t *launches, double *total_ms, double *total_bytes);
 
 #ifdef __cplusplus
 }

@@ -187,13 +187,20 @@ def test_ldc2d_gmres_jacobi_matches_oracle():
     assert max(abs(a - b) for a, b in zip(its_gpu, its_ref)) <= 2, (its_gpu, its_ref)
 
 
-def test_ldc3d_small_matches_oracle():
+@pytest.mark.parametrize("rtol,bound", [(1e-12, 1e-8), (1e-10, 1e-7)])
+def test_ldc3d_small_matches_oracle(rtol, bound):
+    """hex8 cavity 6^3, 3 steps, GMRES(200)+Jacobi on both sides.
+
+    The two runs solve each step's linear system to the same relative
+    preconditioned-residual tolerance, so their answers may differ by about
+    cond(A)*rtol: at rtol 1e-10 that is ~2e-8 here (bound 1e-7), at 1e-12 the
+    1e-8 field bound holds."""
     mesh, ctrl, _ = meshgen.case_hex(6, 3)
-    ref = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=200, rtol=1e-10, pc="jacobi", threads=4)
+    ref = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=200, rtol=rtol, pc="jacobi", threads=4)
     ref.solve()
-    s, stats = _run_gpu(mesh, ctrl, restart=200, rtol=1e-10, pc="jacobi")
+    s, stats = _run_gpu(mesh, ctrl, restart=200, rtol=rtol, pc="jacobi")
     rel = np.linalg.norm(s - ref.soln) / np.linalg.norm(ref.soln)
-    assert rel < 1e-8, rel
+    assert rel < bound, rel
     its_gpu = [st["ksp_its"] for st in stats]
     its_ref = [st["gmres_its"] for st in ref.stats]
     assert its_gpu and all(len(a) == len(b) for a, b in zip(its_gpu, its_ref))
