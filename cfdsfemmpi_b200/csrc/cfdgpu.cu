@@ -62,6 +62,7 @@ struct cfdgpu_handle {
   double *bsr = nullptr;
   double *dinv = nullptr, *binv = nullptr;
   int m = 0;
+  int64_t ldv = 0;     // Krylov vector stride (multiple of 32 doubles, zero padded)
   double *V = nullptr;
   GmresState *gst = nullptr;
   GmresArrays ga{};
@@ -410,7 +411,9 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
 {
   const int64_t n = h->n;
   const int m = h->m;
-  const int64_t ldv = n;
+  const int64_t ldv = h->ldv;
+  const int64_t npair = ldv / 2;
+  const int ntiles = (int)((npair + ORTHO_THREADS - 1) / ORTHO_THREADS);
   double *V = h->V;
   GmresState *st = h->gst;
   int rc;
@@ -422,6 +425,7 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
   else pc_apply<3><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, V);
   LAUNCHED(h);
   const int vgrid = grid_for(n);
+  const int pgrid = grid_for(npair);
   while (true) {
     gmres_start<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, st, h->ga);
     scale_v0<<<vgrid, 256, 0, h->stream>>>(n, V, st);
@@ -430,36 +434,32 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
     // Arnoldi steps; poll the device flag one chunk behind so the GPU stays fed
     const int CH = 8;
     bool stop = false;
-    int polled_chunk = -1;
     cudaEvent_t evs[2] = {h->ev0, h->ev1};
     for (int j0 = 0; j0 < m && !stop; j0 += CH) {
       for (int j = j0; j < std::min(m, j0 + CH); j++) {
         if ((rc = spmv_pc(h, 0, V + (int64_t)j * ldv, nullptr, V + (int64_t)(j + 1) * ldv, st, j))) return rc;
-        dim3 g2(RED_BLOCKS, (j + 1 + MDOT_CHUNK - 1) / MDOT_CHUNK);
-        // multi-dot reads V_0..V_j and w; update reads them again and writes w
         const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 5.0) * 8.0 * n);
-        gmres_mdot<<<g2, RED_THREADS, 0, h->stream>>>(n, V, ldv, j, st, h->ga);
-        gmres_maxpy_norm<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, ldv, j, st, h->ga);
+        dim3 g2(ntiles, (j + 1 + MDOT_KC - 1) / MDOT_KC);
+        gmres_mdot<<<g2, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga.partial);
+        gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, h->ga.partial, h->ga.H);
+        gmres_maxpy_norm<<<ntiles, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga);
         prof_end(h, pi);
-        gmres_scale_next<<<vgrid, 256, 0, h->stream>>>(n, V, ldv, j, st);
-        h->launches += 3;
+        gmres_scale_next<<<pgrid, 256, 0, h->stream>>>(npair, V, ldv, j, st);
+        h->launches += 4;
       }
       if ((rc = check_launch(h, "gmres_arnoldi"))) return rc;
       const int cidx = (j0 / CH) & 1;
       CK(cudaMemcpyAsync(&h->h_gst[cidx], st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
       CK(cudaEventRecord(evs[cidx], h->stream));
       // wait for the previous chunk's snapshot
-      if (polled_chunk >= 0 || j0 > 0) {
-        const int pidx = ((j0 / CH) - 1) & 1;
-        if (j0 > 0) {
-          CK(cudaEventSynchronize(evs[pidx]));
-          if (!h->h_gst[pidx].active) stop = true;
-        }
+      if (j0 > 0) {
+        const int pidx = cidx ^ 1;
+        CK(cudaEventSynchronize(evs[pidx]));
+        if (!h->h_gst[pidx].active) stop = true;
       }
-      polled_chunk = j0 / CH;
     }
-    gmres_backsub<<<1, 32, 0, h->stream>>>(st, h->ga);
-    gmres_update_x<<<vgrid, 256, 0, h->stream>>>(n, x, V, ldv, st, h->ga);
+    gmres_backsub<<<1, 1024, 0, h->stream>>>(st, h->ga);
+    gmres_update_x<<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, V, ldv, st, h->ga);
     h->launches += 2;
     if ((rc = check_launch(h, "gmres_build_soln"))) return rc;
     CK(cudaMemcpyAsync(h->h_gst, st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
@@ -572,14 +572,19 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
   if ((rc = dalloc(h, &h->dinv, (size_t)n))) return rc;
   if ((rc = dalloc(h, &h->binv, (size_t)h->nNode * bb))) return rc;
-  if ((rc = dalloc(h, &h->V, (size_t)n * (h->m + 1)))) return rc;
+  h->ldv = (n + 31) / 32 * 32;
+  if ((rc = dalloc(h, &h->V, (size_t)h->ldv * (h->m + 1)))) return rc;
+  CK(cudaMemset(h->V, 0, sizeof(double) * h->ldv * (h->m + 1)));
   if ((rc = dalloc(h, &h->gst, 1))) return rc;
   if ((rc = dalloc(h, &h->ga.H, (size_t)(h->m + 1) * h->m))) return rc;
   if ((rc = dalloc(h, &h->ga.cs, (size_t)h->m))) return rc;
   if ((rc = dalloc(h, &h->ga.sn, (size_t)h->m))) return rc;
   if ((rc = dalloc(h, &h->ga.grs, (size_t)h->m + 1))) return rc;
   if ((rc = dalloc(h, &h->ga.y, (size_t)h->m))) return rc;
-  if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * RED_BLOCKS))) return rc;
+  {
+    const int64_t ntiles = (h->ldv / 2 + ORTHO_THREADS - 1) / ORTHO_THREADS;
+    if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
+  }
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
   if ((rc = dalloc(h, &h->red_counter, 1))) return rc;
   CK(cudaMemset(h->red_counter, 0, sizeof(unsigned int)));

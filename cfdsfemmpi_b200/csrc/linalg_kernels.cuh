@@ -5,9 +5,10 @@
 // preconditioned-residual norm, KSPConvergedDefault; the reference calls it
 // from src/base/SolverPetsc.cpp:253).
 //
-// Determinism: every reduction uses a fixed grid (RED_BLOCKS CTAs), a fixed
-// per-thread stride, a fixed in-CTA tree, and a last-CTA pass that adds the
-// per-CTA partials in index order, so results do not depend on scheduling.
+// Determinism: every reduction uses a fixed grid, a fixed per-thread stride,
+// a fixed in-CTA tree, and a final pass (last CTA, or one warp per output)
+// that adds the per-CTA partials in index order, so results do not depend on
+// scheduling.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -16,7 +17,6 @@ namespace cfdgpu {
 
 constexpr int RED_BLOCKS = 296;     // 2 x 148 SMs
 constexpr int RED_THREADS = 256;
-constexpr int MDOT_CHUNK = 8;       // basis vectors per CTA row in the multi-dot
 
 // ---------------------------------------------------------------------------
 // GMRES control block (device memory).  One thread (the last CTA of a
@@ -37,11 +37,11 @@ struct GmresState {
 };
 
 struct GmresArrays {
-  double *H;       // (m+1) x m, row-major H[r*m + c]
+  double *H;       // (m+1) x m, column-major, see hidx()
   double *cs, *sn; // m
   double *grs;     // m+1
   double *y;       // m
-  double *partial; // scratch for reductions: (m+1) * RED_BLOCKS doubles
+  double *partial; // scratch for reductions: (m+1) * ntiles doubles
 };
 
 __device__ __forceinline__ int ksp_converged(GmresState *s, int n_its, double rnorm)
@@ -317,85 +317,136 @@ __global__ void scale_v0(int64_t n, double *__restrict__ v0, const GmresState *_
     v0[i] *= s;
 }
 
-// h_k = <w, V_k>, k = 0..j (classical Gram-Schmidt dot products).
-// grid: (RED_BLOCKS, ceil((j+1)/MDOT_CHUNK)).  The last CTA writes H[k][j].
-__global__ void __launch_bounds__(RED_THREADS)
-gmres_mdot(int64_t n, const double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
+// Hessenberg storage: column-major, leading dimension m+1: H(r, c) = H[c*(m+1) + r].
+__device__ __forceinline__ int64_t hidx(int r, int c, int m) { return (int64_t)c * (m + 1) + r; }
+
+// Krylov vectors are stored with a leading dimension ldv that is a multiple
+// of 32 doubles; entries n..ldv-1 stay zero, so every kernel below processes
+// pairs of doubles (16-byte loads) over npair = ldv/2.
+constexpr int ORTHO_THREADS = 256;
+constexpr int MDOT_KC = 8;          // basis vectors per CTA in the multi-dot
+
+__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+
+// Classical Gram-Schmidt dot products, pass 1: per column tile partial sums
+// of <w, V_k> for a chunk of MDOT_KC vectors.  grid (ntiles, ceil((j+1)/KC)).
+__global__ void __launch_bounds__(ORTHO_THREADS)
+gmres_mdot(int64_t npair, const double *__restrict__ V, int64_t ldv, int j, const GmresState *__restrict__ st,
+           double *__restrict__ partial)
 {
   if (!st->active || st->it != j) return;
-  __shared__ double sh[RED_THREADS / 32];
-  const int k0 = blockIdx.y * MDOT_CHUNK;
-  const int nk = min(MDOT_CHUNK, j + 1 - k0);
+  __shared__ double sh[MDOT_KC][ORTHO_THREADS / 32];
+  const int k0 = blockIdx.y * MDOT_KC;
+  const int nk = min(MDOT_KC, j + 1 - k0);
+  const int64_t p = (int64_t)blockIdx.x * ORTHO_THREADS + threadIdx.x;
   const double *w = V + (int64_t)(j + 1) * ldv;
-  double s[MDOT_CHUNK];
+  double acc[MDOT_KC];
 #pragma unroll
-  for (int q = 0; q < MDOT_CHUNK; q++) s[q] = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
-    const double wi = w[i];
+  for (int q = 0; q < MDOT_KC; q++) acc[q] = 0.0;
+  if (p < npair) {
+    const double2 wv = ld2(w + 2 * p);
 #pragma unroll
-    for (int q = 0; q < MDOT_CHUNK; q++)
-      if (q < nk) s[q] = fma(wi, V[(int64_t)(k0 + q) * ldv + i], s[q]);
-  }
-#pragma unroll
-  for (int q = 0; q < MDOT_CHUNK; q++) {
-    if (q < nk) {
-      const double t = block_sum<RED_THREADS>(s[q], sh);
-      if (threadIdx.x == 0) ga.partial[(int64_t)(k0 + q) * gridDim.x + blockIdx.x] = t;
+    for (int q = 0; q < MDOT_KC; q++) {
+      if (q < nk) {
+        const double2 v = ld2(V + (int64_t)(k0 + q) * ldv + 2 * p);
+        acc[q] = fma(wv.x, v.x, wv.y * v.y);
+      }
     }
   }
-  if (last_block(&st->counter, gridDim.x * gridDim.y)) {
-    const int m = st->m;
-    for (int k = threadIdx.x; k <= j; k += blockDim.x) {
-      double t = 0.0;
-      for (unsigned int b = 0; b < gridDim.x; b++) t += ga.partial[(int64_t)k * gridDim.x + b];
-      ga.H[(int64_t)k * m + j] = t;
-    }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < MDOT_KC; q++) {
+    double v = acc[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[q][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < nk) {
+    double t = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < ORTHO_THREADS / 32; w2++) t += sh[threadIdx.x][w2];
+    partial[(int64_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = t;
   }
 }
 
-// w -= sum_k H[k][j] V_k, then ||w||, Hessenberg/Givens update and the
-// convergence test (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
-__global__ void __launch_bounds__(RED_THREADS)
-gmres_maxpy_norm(int64_t n, double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
+// pass 2: one warp per k sums the tile partials in a fixed order -> H(k, j)
+__global__ void gmres_mdot_reduce(int ntiles, int j, const GmresState *__restrict__ st,
+                                  const double *__restrict__ partial, double *__restrict__ H)
 {
   if (!st->active || st->it != j) return;
-  __shared__ double sh[RED_THREADS / 32];
+  const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (k > j) return;
+  const double *pp = partial + (int64_t)k * ntiles;
+  double t = 0.0;
+  for (int b = lane; b < ntiles; b += 32) t += pp[b];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) H[hidx(k, j, st->m)] = t;
+}
+
+// w -= sum_k H(k, j) V_k (pairs of columns per thread, loads unrolled by 4),
+// per-tile ||w||^2; the last tile finishes the norm, applies the stored
+// Givens rotations to column j, forms the new one and runs the convergence
+// test (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
+__global__ void __launch_bounds__(ORTHO_THREADS)
+gmres_maxpy_norm(int64_t npair, double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
+{
+  if (!st->active || st->it != j) return;
   __shared__ double hk[1024];
+  __shared__ double sh[ORTHO_THREADS / 32];
   const int m = st->m;
-  for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[(int64_t)k * m + j];
+  for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[hidx(k, j, m)];
   __syncthreads();
   double *w = V + (int64_t)(j + 1) * ldv;
+  const int64_t p = (int64_t)blockIdx.x * ORTHO_THREADS + threadIdx.x;
   double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
-    double wi = w[i];
-    for (int k = 0; k <= j; k++) wi = fma(-hk[k], V[(int64_t)k * ldv + i], wi);
-    w[i] = wi;
-    s = fma(wi, wi, s);
+  if (p < npair) {
+    double2 a = ld2(w + 2 * p);
+    int k = 0;
+    for (; k + 4 <= j + 1; k += 4) {
+      const double2 v0 = ld2(V + (int64_t)(k + 0) * ldv + 2 * p);
+      const double2 v1 = ld2(V + (int64_t)(k + 1) * ldv + 2 * p);
+      const double2 v2 = ld2(V + (int64_t)(k + 2) * ldv + 2 * p);
+      const double2 v3 = ld2(V + (int64_t)(k + 3) * ldv + 2 * p);
+      a.x = fma(-hk[k], v0.x, a.x); a.y = fma(-hk[k], v0.y, a.y);
+      a.x = fma(-hk[k + 1], v1.x, a.x); a.y = fma(-hk[k + 1], v1.y, a.y);
+      a.x = fma(-hk[k + 2], v2.x, a.x); a.y = fma(-hk[k + 2], v2.y, a.y);
+      a.x = fma(-hk[k + 3], v3.x, a.x); a.y = fma(-hk[k + 3], v3.y, a.y);
+    }
+    for (; k <= j; k++) {
+      const double2 v0 = ld2(V + (int64_t)k * ldv + 2 * p);
+      a.x = fma(-hk[k], v0.x, a.x); a.y = fma(-hk[k], v0.y, a.y);
+    }
+    *reinterpret_cast<double2 *>(w + 2 * p) = a;
+    s = fma(a.x, a.x, a.y * a.y);
   }
-  s = block_sum<RED_THREADS>(s, sh);
+  s = block_sum<ORTHO_THREADS>(s, sh);
   if (threadIdx.x == 0) ga.partial[blockIdx.x] = s;
   if (last_block(&st->counter, gridDim.x)) {
+    double t = 0.0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += ORTHO_THREADS) t += ga.partial[b];
+    t = block_sum<ORTHO_THREADS>(t, sh);
     if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (unsigned int b = 0; b < gridDim.x; b++) t += ga.partial[b];
       const double tt = sqrt(t);
       st->tt = tt;
       double *H = ga.H;
       const int it = j;
-      H[(int64_t)(it + 1) * m + it] = tt;
+      H[hidx(it + 1, it, m)] = tt;
       double hapbnd = fabs(tt / ga.grs[it]);
       if (hapbnd > 1.0e-30) hapbnd = 1.0e-30;
       const bool hapend = tt < hapbnd;
       for (int q = 1; q <= it; q++) {
-        const double a = H[(int64_t)(q - 1) * m + it];
-        const double bq = H[(int64_t)q * m + it];
-        H[(int64_t)(q - 1) * m + it] = ga.cs[q - 1] * a + ga.sn[q - 1] * bq;
-        H[(int64_t)q * m + it] = ga.cs[q - 1] * bq - ga.sn[q - 1] * a;
+        const double a = H[hidx(q - 1, it, m)];
+        const double bq = H[hidx(q, it, m)];
+        H[hidx(q - 1, it, m)] = ga.cs[q - 1] * a + ga.sn[q - 1] * bq;
+        H[hidx(q, it, m)] = ga.cs[q - 1] * bq - ga.sn[q - 1] * a;
       }
       double res;
       int reason = 0;
       if (!hapend) {
-        const double a = H[(int64_t)it * m + it], bq = H[(int64_t)(it + 1) * m + it];
+        const double a = H[hidx(it, it, m)], bq = H[hidx(it + 1, it, m)];
         const double r = sqrt(a * a + bq * bq);
         if (r == 0.0) {
           reason = -2;   // KSP_DIVERGED_NULL
@@ -405,7 +456,7 @@ gmres_maxpy_norm(int64_t n, double *__restrict__ V, int64_t ldv, int j, GmresSta
           ga.sn[it] = bq / r;
           ga.grs[it + 1] = -(ga.sn[it] * ga.grs[it]);
           ga.grs[it] = ga.cs[it] * ga.grs[it];
-          H[(int64_t)it * m + it] = ga.cs[it] * a + ga.sn[it] * bq;
+          H[hidx(it, it, m)] = ga.cs[it] * a + ga.sn[it] * bq;
           res = fabs(ga.grs[it + 1]);
         }
       } else {
@@ -425,44 +476,58 @@ gmres_maxpy_norm(int64_t n, double *__restrict__ V, int64_t ldv, int j, GmresSta
 }
 
 // V_{j+1} /= tt (VecNormalize), only if step j ran
-__global__ void gmres_scale_next(int64_t n, double *__restrict__ V, int64_t ldv, int j, const GmresState *__restrict__ st)
+__global__ void gmres_scale_next(int64_t npair, double *__restrict__ V, int64_t ldv, int j,
+                                 const GmresState *__restrict__ st)
 {
   if (st->it != j + 1) return;
   const double tt = st->tt;
   if (tt == 0.0) return;
   const double s = 1.0 / tt;
   double *w = V + (int64_t)(j + 1) * ldv;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    w[i] *= s;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair; p += (int64_t)gridDim.x * blockDim.x) {
+    double2 a = ld2(w + 2 * p);
+    a.x *= s; a.y *= s;
+    *reinterpret_cast<double2 *>(w + 2 * p) = a;
+  }
 }
 
-// KSPGMRESBuildSoln: back substitution for the it x it triangular system.
-__global__ void gmres_backsub(GmresState *st, GmresArrays ga)
+// KSPGMRESBuildSoln back substitution, column-oriented: one CTA; for k from
+// the last column down, y_k = r_k / H(k,k), then r_i -= H(i,k) y_k for i < k.
+__global__ void __launch_bounds__(1024) gmres_backsub(GmresState *st, GmresArrays ga)
 {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ double r[1024];
+  __shared__ double yk;
   const int last = st->it - 1;
   const int m = st->m;
   if (last < 0) return;
-  const double *H = ga.H;
-  double *y = ga.y;
-  y[last] = (H[(int64_t)last * m + last] != 0.0) ? ga.grs[last] / H[(int64_t)last * m + last] : 0.0;
-  for (int ii = 1; ii <= last; ii++) {
-    const int k = last - ii;
-    double t = ga.grs[k];
-    for (int q = k + 1; q <= last; q++) t = t - H[(int64_t)k * m + q] * y[q];
-    y[k] = (H[(int64_t)k * m + k] != 0.0) ? t / H[(int64_t)k * m + k] : 0.0;
+  for (int i = threadIdx.x; i <= last; i += blockDim.x) r[i] = ga.grs[i];
+  __syncthreads();
+  for (int k = last; k >= 0; k--) {
+    if (threadIdx.x == 0) {
+      const double d = ga.H[hidx(k, k, m)];
+      yk = (d != 0.0) ? r[k] / d : 0.0;
+      ga.y[k] = yk;
+    }
+    __syncthreads();
+    const double y = yk;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) r[i] -= ga.H[hidx(i, k, m)] * y;
+    __syncthreads();
   }
 }
 
 // x += sum_{k < it} y_k V_k
-__global__ void gmres_update_x(int64_t n, double *__restrict__ x, const double *__restrict__ V, int64_t ldv,
-                               const GmresState *__restrict__ st, GmresArrays ga)
+__global__ void __launch_bounds__(ORTHO_THREADS)
+gmres_update_x(int64_t n, double *__restrict__ x, const double *__restrict__ V, int64_t ldv,
+               const GmresState *__restrict__ st, GmresArrays ga)
 {
+  __shared__ double yk[1024];
   const int it = st->it;
   if (it <= 0) return;
+  for (int k = threadIdx.x; k < it; k += blockDim.x) yk[k] = ga.y[k];
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int k = 0; k < it; k++) s = fma(ga.y[k], V[(int64_t)k * ldv + i], s);
+    for (int k = 0; k < it; k++) s = fma(yk[k], V[(int64_t)k * ldv + i], s);
     x[i] += s;
   }
 }
