@@ -20,7 +20,7 @@ EXPORTS = [
     "cfdgpu_set_solution", "cfdgpu_device_solution", "cfdgpu_stream", "cfdgpu_set_history", "cfdgpu_get_history",
     "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
     "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
-    "cfdgpu_set_profiling", "cfdgpu_kernel_stats",
+    "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual",
 ]
 KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
 
@@ -104,6 +104,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_assemble_export.argtypes = [vp, ip, vp, vp]
     L.cfdgpu_solve_export.argtypes = [vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.cfdgpu_timers.argtypes = [vp, vp]
+    L.cfdgpu_true_residual.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
     L.cfdgpu_set_profiling.argtypes = [vp, ip]
@@ -292,6 +293,13 @@ class Handle:
         its, reason = ctypes.c_int(), ctypes.c_int()
         self._check(self._L.cfdgpu_solve_export(self.h, _ptr(bb), _ptr(x), ctypes.byref(its), ctypes.byref(reason)))
         return x, its.value, reason.value
+
+    def true_residual(self, x: np.ndarray, b: np.ndarray) -> float:
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        out = ctypes.c_double()
+        self._check(self._L.cfdgpu_true_residual(self.h, _ptr(xx), _ptr(bb), ctypes.byref(out)))
+        return float(out.value)
 
     def timers(self) -> np.ndarray:
         t = np.zeros(5)

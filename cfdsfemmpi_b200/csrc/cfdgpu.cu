@@ -833,6 +833,21 @@ int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, 
   return 0;
 }
 
+int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm)
+{
+  if (!h || !x || !b || !norm) return CFDGPU_EINVAL;
+  if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
+  // x -> dx, b -> rhs, r = b - A x -> applied-free scratch (the Krylov vector V_0)
+  CK(cudaMemcpyAsync(h->dx, x, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->rhs, b, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  const int saved_pc = h->opts.pc_type;
+  h->opts.pc_type = CFDGPU_PC_NONE;
+  int rc = spmv_pc(h, 1, h->dx, h->rhs, h->V, nullptr, 0);
+  h->opts.pc_type = saved_pc;
+  if (rc) return rc;
+  return norm2(h, h->V, norm);
+}
+
 int cfdgpu_timers(cfdgpu_handle *h, double t[5])
 {
   if (!h || !t) return CFDGPU_EINVAL;

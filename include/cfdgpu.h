@@ -187,6 +187,11 @@ int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double 
  * dofs).  its/reason may be NULL. */
 int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, int *reason);
 
+/* True (unpreconditioned) residual of the last assembled system:
+ * *norm = ||b - A x||_2 with the library's deterministic reduction.  x and b
+ * are host arrays of nNode*ndof doubles (zero at Dirichlet dofs). */
+int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm);
+
 /* Timers in the reference's categories (StabFEM::printComputerTimes,
  * StabFEM.cpp:711-727), seconds: [0] pattern, [1] assembly, [2] solver,
  * [3] post-process (unused by the library), [4] total in cfdgpu_step. */

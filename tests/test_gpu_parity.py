@@ -248,3 +248,27 @@ def test_kat_ldc2dquad_mesh2_through_driver(golden_dir):
     diff = np.abs(io.read_result(ref) - fem.solution().reshape(-1, 3)).max()
     assert diff < 1e-6
     fem.deallocatePetscObjects()
+
+
+def test_true_residual_matches_host():
+    """||b - A x|| on the device equals the host computation on the exported BSR."""
+    mesh = MESHES["hex8"]()
+    ctrl = meshgen.control_for(5, 0.1, 0.001)
+    prev, cur, dot = _random_state(mesh.nNode * mesh.ndof, 9)
+    h = Handle(mesh, ctrl)
+    h.set_element_state(prev, cur, dot)
+    vals, rhs = h.assemble_export(0)
+    d = h.export_pattern()
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(h.n)
+    x[d["fixed_dofs"]] = 0.0
+    dev = h.true_residual(x, rhs)
+    rowptr, colidx = d["rowptr"], d["colidx"]
+    xb = x.reshape(-1, 4)
+    y = np.zeros_like(xb)
+    for r in range(mesh.nNode):
+        for k in range(rowptr[r], rowptr[r + 1]):
+            y[r] += vals[k] @ xb[colidx[k]]
+    host = np.linalg.norm(rhs - y.ravel())
+    h.close()
+    assert abs(dev - host) <= 1e-12 * host
