@@ -234,22 +234,6 @@ def test_kat_ldc2dquad10_through_driver(golden_dir, tmp_path):
     fem.deallocatePetscObjects()
 
 
-@pytest.mark.slow
-def test_kat_ldc2dquad_mesh2_through_driver(golden_dir):
-    d = os.path.join(golden_dir, "ldc2dquad-mesh2")
-    fem = StabFEM()
-    fem.readInputData(os.path.join(d, "LDC2Dquad-mesh2"))
-    fem.readControlParameters(os.path.join(d, "control-parameters-Re1000.dat"))
-    fem.write_forces = False
-    fem.setSolver(1, None, False, options=os.path.join(d, "petsc_options.dat"))
-    assert fem.solveFullyImplicit() == 0
-    ref = os.path.join(d, "test-ldc-stru-mesh2-ref.dat")
-    assert fem.checkResult(ref) == 0
-    diff = np.abs(io.read_result(ref) - fem.solution().reshape(-1, 3)).max()
-    assert diff < 1e-6
-    fem.deallocatePetscObjects()
-
-
 def test_true_residual_matches_host():
     """||b - A x|| on the device equals the host computation on the exported BSR."""
     mesh = MESHES["hex8"]()
