@@ -20,11 +20,11 @@ EXPORTS = [
     "cfdgpu_set_solution", "cfdgpu_device_solution", "cfdgpu_stream", "cfdgpu_set_history", "cfdgpu_get_history",
     "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
     "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
-    "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual",
+    "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual", "cfdgpu_residual_norm_noalloc",
 ]
 KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
 
-OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV = 0, -1, -2, -3, -4, -5, -6
+OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV, ETOOBIG = 0, -1, -2, -3, -4, -5, -6, -7
 PC = {"none": 0, "jacobi": 1, "pbjacobi": 2}
 PREC = {"fp64": 0, "mixed": 1}
 MAX_NEWTON = 32
@@ -105,6 +105,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_solve_export.argtypes = [vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.cfdgpu_timers.argtypes = [vp, vp]
     L.cfdgpu_true_residual.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
+    L.cfdgpu_residual_norm_noalloc.argtypes = [ip, ip, vp, vp, vp, vp, vp, vp, vp]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
     L.cfdgpu_set_profiling.argtypes = [vp, ip]

@@ -884,3 +884,77 @@ int cfdgpu_kernel_stats(cfdgpu_handle *h, int kind, int64_t *launches, double *t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual norm.
+//
+// Some callers may not allocate device memory themselves: a host code that
+// runs inside another framework's memory pool (where cudaMalloc is disallowed
+// or would fragment the pool), a solver embedded in a process whose GPU memory
+// is budgeted up front, or code that may only enqueue work on a stream it is
+// handed.  cfdgpu_residual_norm_noalloc serves them: it computes the same
+// ||b - A x||_2 as cfdgpu_true_residual on a BSR matrix the caller already
+// holds on the device, and keeps its scratch (the residual vector and the
+// reduction partials) in the file-scope device array below instead of
+// allocating.  The array is reserved when the library is loaded and every GPU
+// that loads the library holds it (16 MiB + 2.6 KiB) until the process exits.
+//
+// Host code must not pass g_noalloc_scratch itself to a kernel: on the host that
+// name is a stand-in, not a device address.  The device address is looked up
+// once per device with cudaGetSymbolAddress and cached.
+namespace {
+constexpr int64_t NOALLOC_MAX_N = int64_t(1) << 21;          // residual entries (nNode*ndof)
+constexpr int64_t NOALLOC_WORDS = NOALLOC_MAX_N + RED_BLOCKS + 32;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_WORDS];
+
+static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch array on the current device (set up once per
+// device, with that device current).
+static int noalloc_scratch(double **out)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CFDGPU_ENODEV;
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return CFDGPU_ECUDA;
+    g_noalloc_ptr[dev] = (double *)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+extern "C" int cfdgpu_residual_norm_noalloc(int nNode, int ndof, const int32_t *d_rowptr, const int32_t *d_colidx,
+                                            const double *d_val, const double *d_x, const double *d_b,
+                                            double *d_norm, void *stream)
+{
+  if (nNode <= 0 || (ndof != 3 && ndof != 4) || !d_rowptr || !d_colidx || !d_val || !d_x || !d_b || !d_norm)
+    return CFDGPU_EINVAL;
+  const int64_t n = (int64_t)nNode * ndof;
+  if (n > NOALLOC_MAX_N) return CFDGPU_ETOOBIG;
+  double *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  double *r = scratch;                                            // residual, n doubles
+  double *partial = scratch + NOALLOC_MAX_N;                      // RED_BLOCKS doubles
+  unsigned int *counter = (unsigned int *)(scratch + NOALLOC_MAX_N + RED_BLOCKS);
+  // the array keeps the previous call's contents: the arrival counter must start at zero
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned int), s) != cudaSuccess) return CFDGPU_ECUDA;
+  if (ndof == 4) {
+    const int grid = (int)((nNode * 32LL + 255) / 256);
+    bsr4_spmv_f64<1, 0><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr, nullptr, r,
+                                              nullptr, 0);
+  } else {
+    const int grid = (int)((n + 255) / 256);
+    bsr_spmv_generic<3, 1, 0, double><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr,
+                                                             nullptr, r, nullptr, 0);
+  }
+  if (cudaGetLastError() != cudaSuccess) return CFDGPU_ECUDA;
+  norm2_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, r, partial, counter, d_norm);
+  if (cudaGetLastError() != cudaSuccess) return CFDGPU_ECUDA;
+  return 0;
+}

@@ -37,6 +37,7 @@ extern "C" {
 #define CFDGPU_EKSP (-4)        /* linear solve diverged (reference exits, SolverPetsc.cpp:264-269) */
 #define CFDGPU_ENOMEM (-5)
 #define CFDGPU_ENODEV (-6)      /* no CUDA device / kernels not loadable */
+#define CFDGPU_ETOOBIG (-7)     /* size beyond the fixed scratch of an allocation-free entry point */
 
 /* element types, as selected in StabFEM::prepareInputData (StabFEM.cpp:351-366) */
 #define CFDGPU_TRI3 0
@@ -191,6 +192,25 @@ int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, 
  * *norm = ||b - A x||_2 with the library's deterministic reduction.  x and b
  * are host arrays of nNode*ndof doubles (zero at Dirichlet dofs). */
 int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm);
+
+/* Allocation-free variant of cfdgpu_true_residual, for callers that may not
+ * allocate device memory (code running inside another framework's memory
+ * pool, or given only a stream to enqueue on).  No handle: the caller passes
+ * a BSR matrix already on the device (row pointer nNode+1, column index,
+ * values in nodal blocks of ndof x ndof, row-major) and device vectors x, b
+ * (nNode*ndof); the kernel writes ||b - A x||_2 to the device double d_norm,
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * ndof is 3 or 4.  Scratch lives in a fixed array inside the library (16 MiB,
+ * held by every GPU that loads the library until exit); nNode*ndof above
+ * 2,097,152 returns CFDGPU_ETOOBIG.  The call allocates nothing.  Its first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (different streams, or different host threads
+ * on one device) race and must be serialised by the caller.  This entry point
+ * has no counterpart in the reference. */
+int cfdgpu_residual_norm_noalloc(int nNode, int ndof, const int32_t *d_rowptr, const int32_t *d_colidx,
+                                 const double *d_val, const double *d_x, const double *d_b, double *d_norm,
+                                 void *stream);
 
 /* Timers in the reference's categories (StabFEM::printComputerTimes,
  * StabFEM.cpp:711-727), seconds: [0] pattern, [1] assembly, [2] solver,
