@@ -414,6 +414,7 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
   const int64_t ldv = h->ldv;
   const int64_t npair = ldv / 2;
   const int ntiles = (int)((npair + ORTHO_THREADS - 1) / ORTHO_THREADS);
+  const int mtiles = (int)((npair + MAXPY_PAIRS - 1) / MAXPY_PAIRS);
   double *V = h->V;
   GmresState *st = h->gst;
   int rc;
@@ -442,7 +443,7 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
         dim3 g2(ntiles, (j + 1 + MDOT_KC - 1) / MDOT_KC);
         gmres_mdot<<<g2, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga.partial);
         gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, h->ga.partial, h->ga.H);
-        gmres_maxpy_norm<<<ntiles, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga);
+        gmres_maxpy_norm<<<mtiles, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga);
         prof_end(h, pi);
         gmres_scale_next<<<pgrid, 256, 0, h->stream>>>(npair, V, ldv, j, st);
         h->launches += 4;
@@ -582,7 +583,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   if ((rc = dalloc(h, &h->ga.grs, (size_t)h->m + 1))) return rc;
   if ((rc = dalloc(h, &h->ga.y, (size_t)h->m))) return rc;
   {
-    const int64_t ntiles = (h->ldv / 2 + ORTHO_THREADS - 1) / ORTHO_THREADS;
+    const int64_t ntiles = (h->ldv / 2 + MAXPY_PAIRS - 1) / MAXPY_PAIRS;
     if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
   }
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;

@@ -112,14 +112,32 @@ bsr4_spmv_f64(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__re
   if (warp >= nrows) return;
   const int sub = lane >> 3, q = lane & 7, row = q >> 1, cp = (q & 1) * 2;
   const int kb0 = rowptr[warp], kb1 = rowptr[warp + 1];
-  double acc = 0.0;
-  for (int kb = kb0 + sub; kb < kb1; kb += 4) {
-    const int c = colidx[kb];
-    const double2 a = *reinterpret_cast<const double2 *>(val + (int64_t)kb * 16 + row * 4 + cp);
-    const double2 xv = *reinterpret_cast<const double2 *>(x + (int64_t)c * 4 + cp);
-    acc = fma(a.x, xv.x, acc);
-    acc = fma(a.y, xv.y, acc);
+  double acc0 = 0.0, acc1 = 0.0;
+  // column indices of up to 32 blocks are fetched once per warp and broadcast
+  // by shuffles, so the loop's loads do not wait on an index load.  All loop
+  // bounds are warp-uniform, so every shuffle runs with the full warp.
+  for (int base = kb0; base < kb1; base += 32) {
+    const int nb = min(32, kb1 - base);
+    const int creg = (lane < nb) ? colidx[base + lane] : 0;
+    for (int t0 = 0; t0 < nb; t0 += 8) {
+      const int ta = t0 + sub, tb = t0 + sub + 4;   // <= 27 and <= 31: valid source lanes
+      const int ca = __shfl_sync(0xffffffffu, creg, ta);
+      const int cb = __shfl_sync(0xffffffffu, creg, tb);
+      if (ta < nb) {
+        const double2 a0 = *reinterpret_cast<const double2 *>(val + (int64_t)(base + ta) * 16 + row * 4 + cp);
+        const double2 x0 = *reinterpret_cast<const double2 *>(x + (int64_t)ca * 4 + cp);
+        acc0 = fma(a0.x, x0.x, acc0);
+        acc0 = fma(a0.y, x0.y, acc0);
+      }
+      if (tb < nb) {
+        const double2 a1 = *reinterpret_cast<const double2 *>(val + (int64_t)(base + tb) * 16 + row * 4 + cp);
+        const double2 x1 = *reinterpret_cast<const double2 *>(x + (int64_t)cb * 4 + cp);
+        acc1 = fma(a1.x, x1.x, acc1);
+        acc1 = fma(a1.y, x1.y, acc1);
+      }
+    }
   }
+  double acc = acc0 + acc1;
   acc += __shfl_xor_sync(0xffffffffu, acc, 1);
   acc += __shfl_xor_sync(0xffffffffu, acc, 8);
   acc += __shfl_xor_sync(0xffffffffu, acc, 16);
@@ -386,39 +404,55 @@ __global__ void gmres_mdot_reduce(int ntiles, int j, const GmresState *__restric
   if (lane == 0) H[hidx(k, j, st->m)] = t;
 }
 
-// w -= sum_k H(k, j) V_k (pairs of columns per thread, loads unrolled by 4),
-// per-tile ||w||^2; the last tile finishes the norm, applies the stored
-// Givens rotations to column j, forms the new one and runs the convergence
-// test (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
+// w -= sum_k H(k, j) V_k, then ||w||^2 partials.  A CTA covers MAXPY_PAIRS
+// column pairs; its four thread quarters take the k's congruent to 0..3 mod 4
+// (16-byte loads, consecutive lanes on consecutive pairs), and the quarter
+// sums are combined in a fixed order through shared memory.  The last CTA
+// finishes the norm, applies the stored Givens rotations to column j, forms
+// the new one and runs the convergence test (KSPGMRESUpdateHessenberg,
+// KSPConvergedDefault).
+constexpr int MAXPY_PAIRS = 64;
 __global__ void __launch_bounds__(ORTHO_THREADS)
 gmres_maxpy_norm(int64_t npair, double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
 {
   if (!st->active || st->it != j) return;
   __shared__ double hk[1024];
   __shared__ double sh[ORTHO_THREADS / 32];
+  __shared__ double2 qs[ORTHO_THREADS / MAXPY_PAIRS][MAXPY_PAIRS];
   const int m = st->m;
   for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[hidx(k, j, m)];
   __syncthreads();
   double *w = V + (int64_t)(j + 1) * ldv;
-  const int64_t p = (int64_t)blockIdx.x * ORTHO_THREADS + threadIdx.x;
-  double s = 0.0;
+  const int lp = threadIdx.x % MAXPY_PAIRS;
+  const int quarter = threadIdx.x / MAXPY_PAIRS;
+  const int64_t p = (int64_t)blockIdx.x * MAXPY_PAIRS + lp;
+  double2 acc = make_double2(0.0, 0.0);
   if (p < npair) {
+    const double *base = V + 2 * p;
+    int k = quarter;
+    for (; k + 12 <= j; k += 16) {
+      const double2 v0 = ld2(base + (int64_t)k * ldv);
+      const double2 v1 = ld2(base + (int64_t)(k + 4) * ldv);
+      const double2 v2 = ld2(base + (int64_t)(k + 8) * ldv);
+      const double2 v3 = ld2(base + (int64_t)(k + 12) * ldv);
+      acc.x = fma(hk[k], v0.x, acc.x); acc.y = fma(hk[k], v0.y, acc.y);
+      acc.x = fma(hk[k + 4], v1.x, acc.x); acc.y = fma(hk[k + 4], v1.y, acc.y);
+      acc.x = fma(hk[k + 8], v2.x, acc.x); acc.y = fma(hk[k + 8], v2.y, acc.y);
+      acc.x = fma(hk[k + 12], v3.x, acc.x); acc.y = fma(hk[k + 12], v3.y, acc.y);
+    }
+    for (; k <= j; k += 4) {
+      const double2 v0 = ld2(base + (int64_t)k * ldv);
+      acc.x = fma(hk[k], v0.x, acc.x); acc.y = fma(hk[k], v0.y, acc.y);
+    }
+  }
+  qs[quarter][lp] = acc;
+  __syncthreads();
+  double s = 0.0;
+  if (quarter == 0 && p < npair) {
     double2 a = ld2(w + 2 * p);
-    int k = 0;
-    for (; k + 4 <= j + 1; k += 4) {
-      const double2 v0 = ld2(V + (int64_t)(k + 0) * ldv + 2 * p);
-      const double2 v1 = ld2(V + (int64_t)(k + 1) * ldv + 2 * p);
-      const double2 v2 = ld2(V + (int64_t)(k + 2) * ldv + 2 * p);
-      const double2 v3 = ld2(V + (int64_t)(k + 3) * ldv + 2 * p);
-      a.x = fma(-hk[k], v0.x, a.x); a.y = fma(-hk[k], v0.y, a.y);
-      a.x = fma(-hk[k + 1], v1.x, a.x); a.y = fma(-hk[k + 1], v1.y, a.y);
-      a.x = fma(-hk[k + 2], v2.x, a.x); a.y = fma(-hk[k + 2], v2.y, a.y);
-      a.x = fma(-hk[k + 3], v3.x, a.x); a.y = fma(-hk[k + 3], v3.y, a.y);
-    }
-    for (; k <= j; k++) {
-      const double2 v0 = ld2(V + (int64_t)k * ldv + 2 * p);
-      a.x = fma(-hk[k], v0.x, a.x); a.y = fma(-hk[k], v0.y, a.y);
-    }
+    const double2 q0 = qs[0][lp], q1 = qs[1][lp], q2 = qs[2][lp], q3 = qs[3][lp];
+    a.x -= ((q0.x + q1.x) + (q2.x + q3.x));
+    a.y -= ((q0.y + q1.y) + (q2.y + q3.y));
     *reinterpret_cast<double2 *>(w + 2 * p) = a;
     s = fma(a.x, a.x, a.y * a.y);
   }
