@@ -113,29 +113,12 @@ bsr4_spmv_f64(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__re
   const int sub = lane >> 3, q = lane & 7, row = q >> 1, cp = (q & 1) * 2;
   const int kb0 = rowptr[warp], kb1 = rowptr[warp + 1];
   double acc0 = 0.0, acc1 = 0.0;
-  // column indices of up to 32 blocks are fetched once per warp and broadcast
-  // by shuffles, so the loop's loads do not wait on an index load.  All loop
-  // bounds are warp-uniform, so every shuffle runs with the full warp.
-  for (int base = kb0; base < kb1; base += 32) {
-    const int nb = min(32, kb1 - base);
-    const int creg = (lane < nb) ? colidx[base + lane] : 0;
-    for (int t0 = 0; t0 < nb; t0 += 8) {
-      const int ta = t0 + sub, tb = t0 + sub + 4;   // <= 27 and <= 31: valid source lanes
-      const int ca = __shfl_sync(0xffffffffu, creg, ta);
-      const int cb = __shfl_sync(0xffffffffu, creg, tb);
-      if (ta < nb) {
-        const double2 a0 = *reinterpret_cast<const double2 *>(val + (int64_t)(base + ta) * 16 + row * 4 + cp);
-        const double2 x0 = *reinterpret_cast<const double2 *>(x + (int64_t)ca * 4 + cp);
-        acc0 = fma(a0.x, x0.x, acc0);
-        acc0 = fma(a0.y, x0.y, acc0);
-      }
-      if (tb < nb) {
-        const double2 a1 = *reinterpret_cast<const double2 *>(val + (int64_t)(base + tb) * 16 + row * 4 + cp);
-        const double2 x1 = *reinterpret_cast<const double2 *>(x + (int64_t)cb * 4 + cp);
-        acc1 = fma(a1.x, x1.x, acc1);
-        acc1 = fma(a1.y, x1.y, acc1);
-      }
-    }
+  for (int kb = kb0 + sub; kb < kb1; kb += 4) {
+    const int c = colidx[kb];
+    const double2 a = *reinterpret_cast<const double2 *>(val + (int64_t)kb * 16 + row * 4 + cp);
+    const double2 xv = *reinterpret_cast<const double2 *>(x + (int64_t)c * 4 + cp);
+    acc0 = fma(a.x, xv.x, acc0);
+    acc0 = fma(a.y, xv.y, acc0);
   }
   double acc = acc0 + acc1;
   acc += __shfl_xor_sync(0xffffffffu, acc, 1);
@@ -462,35 +445,45 @@ gmres_maxpy_norm(int64_t npair, double *__restrict__ V, int64_t ldv, int j, Gmre
     double t = 0.0;
     for (unsigned int b = threadIdx.x; b < gridDim.x; b += ORTHO_THREADS) t += ga.partial[b];
     t = block_sum<ORTHO_THREADS>(t, sh);
+    // stage column j of H and the stored rotations in shared memory (hk is
+    // free again), so the serial rotation chain below runs from registers and
+    // shared memory instead of global-memory round trips
+    __shared__ double rc[1024], rs[1024];
+    double *hc = hk;
+    const int it = j;
+    for (int q = threadIdx.x; q <= it; q += blockDim.x) hc[q] = ga.H[hidx(q, it, m)];
+    for (int q = threadIdx.x; q < it; q += blockDim.x) { rc[q] = ga.cs[q]; rs[q] = ga.sn[q]; }
+    __syncthreads();
     if (threadIdx.x == 0) {
       const double tt = sqrt(t);
       st->tt = tt;
-      double *H = ga.H;
-      const int it = j;
-      H[hidx(it + 1, it, m)] = tt;
+      hc[it + 1] = tt;
       double hapbnd = fabs(tt / ga.grs[it]);
       if (hapbnd > 1.0e-30) hapbnd = 1.0e-30;
       const bool hapend = tt < hapbnd;
+      // apply the previous rotations to the new column
+      double a = hc[0];
       for (int q = 1; q <= it; q++) {
-        const double a = H[hidx(q - 1, it, m)];
-        const double bq = H[hidx(q, it, m)];
-        H[hidx(q - 1, it, m)] = ga.cs[q - 1] * a + ga.sn[q - 1] * bq;
-        H[hidx(q, it, m)] = ga.cs[q - 1] * bq - ga.sn[q - 1] * a;
+        const double bq = hc[q];
+        hc[q - 1] = rc[q - 1] * a + rs[q - 1] * bq;
+        a = rc[q - 1] * bq - rs[q - 1] * a;
       }
+      hc[it] = a;
       double res;
       int reason = 0;
       if (!hapend) {
-        const double a = H[hidx(it, it, m)], bq = H[hidx(it + 1, it, m)];
+        const double bq = hc[it + 1];
         const double r = sqrt(a * a + bq * bq);
         if (r == 0.0) {
           reason = -2;   // KSP_DIVERGED_NULL
           res = st->res;
         } else {
-          ga.cs[it] = a / r;
-          ga.sn[it] = bq / r;
-          ga.grs[it + 1] = -(ga.sn[it] * ga.grs[it]);
-          ga.grs[it] = ga.cs[it] * ga.grs[it];
-          H[hidx(it, it, m)] = ga.cs[it] * a + ga.sn[it] * bq;
+          const double c = a / r, sn = bq / r;
+          ga.cs[it] = c;
+          ga.sn[it] = sn;
+          ga.grs[it + 1] = -(sn * ga.grs[it]);
+          ga.grs[it] = c * ga.grs[it];
+          hc[it] = c * a + sn * bq;
           res = fabs(ga.grs[it + 1]);
         }
       } else {
@@ -506,6 +499,8 @@ gmres_maxpy_norm(int64_t npair, double *__restrict__ V, int64_t ldv, int j, Gmre
       st->reason = reason;
       st->active = (reason == 0 && st->it < m && st->its < st->maxit) ? 1 : 0;
     }
+    __syncthreads();
+    for (int q = threadIdx.x; q <= it + 1; q += blockDim.x) ga.H[hidx(q, it, m)] = hc[q];
   }
 }
 
