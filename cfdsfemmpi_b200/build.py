@@ -35,8 +35,32 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in sources() + headers())
 
 
+HOST = os.path.join(HERE, "host")
+BIN = os.path.join(HERE, "bin")
+PROGRAMS = {"cfdsfemmpi": "cfdsfemmpi.cpp", "test-ldc-stru": "test-ldc-stru.cpp"}
+
+
+def build_host(verbose: bool = False) -> None:
+    """The C++ driver (StabFEM) and the reference-shaped command-line programs."""
+    os.makedirs(BIN, exist_ok=True)
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    cuda_lib = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64")
+    deps = [os.path.join(HOST, f) for f in os.listdir(HOST)] + [LIB]
+    for prog, main in PROGRAMS.items():
+        out = os.path.join(BIN, prog)
+        if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-I", inc, "-o", out, os.path.join(HOST, main),
+               os.path.join(HOST, "StabFEM.cpp"), "-L", HERE, "-lcfdgpu", "-L", cuda_lib, "-lcudart",
+               "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
+        build_host(verbose)
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", *sources(), "-lcudart"]
@@ -44,6 +68,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd))
     subprocess.check_call(cmd, cwd=CSRC)
     os.replace(LIB + ".tmp", LIB)
+    build_host(verbose)
     return LIB
 
 
