@@ -62,7 +62,15 @@ struct cfdgpu_handle {
   double *bsr = nullptr;
   double *dinv = nullptr, *binv = nullptr;
   int m = 0;
-  int64_t ldv = 0;     // Krylov vector stride (multiple of 32 doubles, zero padded)
+  int64_t ldv = 0;     // Krylov vector stride (multiple of 32 entries, zero padded)
+  // mixed precision
+  bool mixed = false;
+  float *bsr32 = nullptr, *dinv32 = nullptr, *binv32 = nullptr, *V32 = nullptr, *b32 = nullptr;
+  double *r64 = nullptr, *d64 = nullptr;
+  int m32 = 0;
+  double inner_rtol = 1e-4, abs_target = 0.0;
+  GmresState *gst32 = nullptr;
+  GmresArrays ga32{};
   double *V = nullptr;
   GmresState *gst = nullptr;
   GmresArrays ga{};
@@ -296,9 +304,15 @@ static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, doub
   ElemParams P;
   P.rho = h->ctrl.rho; P.mu = h->ctrl.mu; P.af = h->td[2]; P.am = h->td[1]; P.acceFact = h->td[8];
   P.stab0 = h->ctrl.stab[0]; P.stab1 = h->ctrl.stab[1]; P.stab2 = h->ctrl.stab[2];
-  element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
-      elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
-      h->rhs, outK, outF, h->negjac);
+  if (h->mixed && MODE != MODE_EXPORT) {
+    element_kernel<ET, float, float, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+        elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr32,
+        h->rhs, outK, outF, h->negjac);
+  } else {
+    element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+        elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
+        h->rhs, outK, outF, h->negjac);
+  }
   prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "element_kernel");
@@ -336,7 +350,10 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
   }
   if (want_K && !t.fixed_dofs.empty()) {
     const int nfix = (int)t.fixed_dofs.size();
-    k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
+    if (h->mixed)
+      k_dirichlet_diag<float><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr32);
+    else
+      k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
     LAUNCHED(h);
     int rc = check_launch(h, "dirichlet_diag");
     if (rc) return rc;
@@ -350,27 +367,36 @@ static int build_pc(cfdgpu_handle *h)
   const int pc = h->opts.pc_type;
   if (pc == CFDGPU_PC_NONE) return 0;
   const int g = (h->nNode + 127) / 128;
-  if (h->ndof == 4) build_jacobi<4, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
-  else build_jacobi<3, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
+  if (h->mixed) {
+    build_jacobi<4, float, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr32, h->dinv32, h->binv32, pc);
+  } else if (h->ndof == 4) {
+    build_jacobi<4, double, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
+  } else {
+    build_jacobi<3, double, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
+  }
   LAUNCHED(h);
   return check_launch(h, "build_jacobi");
 }
 
-// y = M^-1 (A x) (mode 0) or y = M^-1 (b - A x) (mode 1)
+static double spmv_bytes(cfdgpu_handle *h, int mode, int vbytes, int mbytes, int pc)
+{
+  // algorithmic bytes: blocks + column indices + row pointers + x + y (+ b)
+  // + the preconditioner's data
+  const double V = (double)vbytes * h->n, B = (double)h->topo.nnzb(), bb = (double)h->ndof * h->ndof;
+  const double pcb = (pc == 1) ? V : (pc == 2) ? (double)vbytes * bb * h->nNode : 0.0;
+  return B * bb * mbytes + 4.0 * B + 4.0 * (h->nNode + 1) + 2.0 * V + (mode == 1 ? V : 0.0) + pcb;
+}
+
+// y = M^-1 (A x) (mode 0) or y = M^-1 (b - A x) (mode 1), FP64 vectors
 static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y, const GmresState *st, int j)
 {
   const int pc = h->opts.pc_type;
-  // algorithmic bytes: blocks + column indices + row pointers + x + y (+ b)
-  // + the preconditioner's data
-  const double V = 8.0 * h->n, B = (double)h->topo.nnzb(), bb = (double)h->ndof * h->ndof;
-  const double pcb = (pc == 1) ? V : (pc == 2) ? 8.0 * bb * h->nNode : 0.0;
-  const int pi = prof_begin(h, CFDGPU_KIND_SPMV, B * bb * 8.0 + 4.0 * B + 4.0 * (h->nNode + 1) + 2.0 * V +
-                                                     (mode == 1 ? V : 0.0) + pcb);
+  const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, mode, 8, 8, pc));
   if (h->ndof == 4) {
     const int grid = (int)((h->nNode * 32LL + 255) / 256);
-#define SPMV4(MO, PCV)                                                                                  \
-  bsr4_spmv_f64<MO, PCV><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, h->dinv, \
-                                                       h->binv, y, st, j)
+#define SPMV4(MO, PCV)                                                                                          \
+  bsr4_spmv<MO, PCV, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, h->dinv, \
+                                                           h->binv, y, st, j)
     if (mode == 0) {
       if (pc == 0) SPMV4(0, 0); else if (pc == 1) SPMV4(0, 1); else SPMV4(0, 2);
     } else {
@@ -394,42 +420,76 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
   return check_launch(h, "bsr_spmv");
 }
 
+// y = M32^-1 (A32 x), FP32 vectors (mixed-precision inner solve)
+static int spmv32_pc(cfdgpu_handle *h, const float *x, float *y, const GmresState *st, int j)
+{
+  const int pc = h->opts.pc_type;
+  const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 0, 4, 4, pc));
+  const int grid = (int)((h->nNode * 32LL + 255) / 256);
+  if (pc == 0)
+    bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j);
+  else if (pc == 1)
+    bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j);
+  else
+    bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j);
+  prof_end(h, pi);
+  LAUNCHED(h);
+  return check_launch(h, "bsr_spmv_f32");
+}
+
+static int norm2_dev(cfdgpu_handle *h, const double *x, double *d_out)
+{
+  norm2_kernel<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(h->n, x, h->red_partial, h->red_counter, d_out);
+  LAUNCHED(h);
+  return check_launch(h, "norm2");
+}
+
 static int norm2(cfdgpu_handle *h, const double *x, double *out_host)
 {
-  norm2_kernel<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(h->n, x, h->red_partial, h->red_counter, h->scalar);
-  LAUNCHED(h);
-  int rc = check_launch(h, "norm2");
+  int rc = norm2_dev(h, x, h->scalar);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(h->h_scalar, h->scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h->h_scalar, h->scalar, sizeof(double) * 1, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   *out_host = h->h_scalar[0];
   return 0;
 }
 
-// Restarted GMRES on the assembled BSR: x = A^-1 b, x0 = 0.
-static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+// One Krylov space: basis, control block and Hessenberg arrays.
+template <typename VT>
+struct Krylov {
+  VT *V = nullptr;
+  int m = 0;
+  int64_t ldv = 0;
+  GmresState *st = nullptr;
+  GmresArrays ga{};
+};
+
+// Restarted GMRES with PETSc semantics on a Krylov space.  The caller has
+// already enqueued V_0 = M^-1 b.  arnoldi(j) enqueues V_{j+1} = M^-1 A V_j;
+// restart() enqueues V_0 = M^-1 (b - A x) (not called when single_cycle).
+// x (FP64) is zeroed here and receives xscale * (the Krylov correction).
+template <typename VT, typename Arn, typename Res>
+static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, double rtol, double atol, double dtol,
+                     bool single_cycle, Arn arnoldi, Res restart, int *its_out, int *reason_out)
 {
+  constexpr int E = Chunk<VT>::E;
   const int64_t n = h->n;
-  const int m = h->m;
-  const int64_t ldv = h->ldv;
-  const int64_t npair = ldv / 2;
-  const int ntiles = (int)((npair + ORTHO_THREADS - 1) / ORTHO_THREADS);
-  const int mtiles = (int)((npair + MAXPY_PAIRS - 1) / MAXPY_PAIRS);
-  double *V = h->V;
-  GmresState *st = h->gst;
+  const int m = K.m;
+  const int64_t ldv = K.ldv;
+  const int64_t nchunk = ldv / E;
+  const int ntiles = (int)((nchunk + ORTHO_THREADS - 1) / ORTHO_THREADS);
+  const int mtiles = (int)((nchunk + MAXPY_CHUNKS - 1) / MAXPY_CHUNKS);
+  VT *V = K.V;
+  GmresState *st = K.st;
   int rc;
-  gmres_init<<<1, 1, 0, h->stream>>>(st, m, h->opts.max_it, h->opts.rtol, h->opts.atol, h->opts.dtol);
+  gmres_init<<<1, 1, 0, h->stream>>>(st, m, max_it, rtol, atol, dtol);
   LAUNCHED(h);
   CK(cudaMemsetAsync(x, 0, sizeof(double) * n, h->stream));
-  // V0 = M^-1 b (x0 = 0)
-  if (h->ndof == 4) pc_apply<4><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, V);
-  else pc_apply<3><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, V);
-  LAUNCHED(h);
   const int vgrid = grid_for(n);
-  const int pgrid = grid_for(npair);
+  const int pgrid = grid_for(nchunk);
   while (true) {
-    gmres_start<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, st, h->ga);
-    scale_v0<<<vgrid, 256, 0, h->stream>>>(n, V, st);
+    gmres_start<VT><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, st, K.ga);
+    scale_v0<VT><<<vgrid, 256, 0, h->stream>>>(n, V, st);
     h->launches += 2;
     if ((rc = check_launch(h, "gmres_start"))) return rc;
     // Arnoldi steps; poll the device flag one chunk behind so the GPU stays fed
@@ -438,14 +498,14 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
     cudaEvent_t evs[2] = {h->ev0, h->ev1};
     for (int j0 = 0; j0 < m && !stop; j0 += CH) {
       for (int j = j0; j < std::min(m, j0 + CH); j++) {
-        if ((rc = spmv_pc(h, 0, V + (int64_t)j * ldv, nullptr, V + (int64_t)(j + 1) * ldv, st, j))) return rc;
-        const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 5.0) * 8.0 * n);
+        if ((rc = arnoldi(j))) return rc;
+        const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 5.0) * (double)sizeof(VT) * n);
         dim3 g2(ntiles, (j + 1 + MDOT_KC - 1) / MDOT_KC);
-        gmres_mdot<<<g2, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga.partial);
-        gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, h->ga.partial, h->ga.H);
-        gmres_maxpy_norm<<<mtiles, ORTHO_THREADS, 0, h->stream>>>(npair, V, ldv, j, st, h->ga);
+        gmres_mdot<VT><<<g2, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga.partial);
+        gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, K.ga.partial, K.ga.H);
+        gmres_maxpy_norm<VT><<<mtiles, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga);
         prof_end(h, pi);
-        gmres_scale_next<<<pgrid, 256, 0, h->stream>>>(npair, V, ldv, j, st);
+        gmres_scale_next<VT><<<pgrid, 256, 0, h->stream>>>(nchunk, V, ldv, j, st);
         h->launches += 4;
       }
       if ((rc = check_launch(h, "gmres_arnoldi"))) return rc;
@@ -459,23 +519,97 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
         if (!h->h_gst[pidx].active) stop = true;
       }
     }
-    gmres_backsub<<<1, 1024, 0, h->stream>>>(st, h->ga);
-    gmres_update_x<<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, V, ldv, st, h->ga);
-    h->launches += 2;
+    gmres_backsub<<<1, 1024, 0, h->stream>>>(st, K.ga);
+    h->launches += 1;
+    gmres_update_x<VT><<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, V, ldv, st, K.ga, 1.0);
+    h->launches += 1;
     if ((rc = check_launch(h, "gmres_build_soln"))) return rc;
     CK(cudaMemcpyAsync(h->h_gst, st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     GmresState s = h->h_gst[0];
     int reason = s.reason;
-    if (reason == 0 && s.its >= h->opts.max_it) reason = -3;   // KSP_DIVERGED_ITS
-    if (reason != 0) {
+    if (reason == 0 && s.its >= max_it) reason = -3;   // KSP_DIVERGED_ITS
+    if (reason != 0 || single_cycle) {
       if (its_out) *its_out = s.its;
       if (reason_out) *reason_out = reason;
       return 0;
     }
-    // restart: V0 = M^-1 (b - A x)
-    if ((rc = spmv_pc(h, 1, x, b, V, nullptr, 0))) return rc;
+    if ((rc = restart())) return rc;
   }
+}
+
+// Restarted GMRES on the assembled FP64 BSR: x = A^-1 b, x0 = 0.
+static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+{
+  const int64_t n = h->n;
+  if (h->ndof == 4)
+    pc_apply<4, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, h->V);
+  else
+    pc_apply<3, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, h->V);
+  LAUNCHED(h);
+  Krylov<double> K;
+  K.V = h->V; K.m = h->m; K.ldv = h->ldv; K.st = h->gst; K.ga = h->ga;
+  auto arn = [&](int j) { return spmv_pc(h, 0, h->V + (int64_t)j * h->ldv, nullptr, h->V + (int64_t)(j + 1) * h->ldv, h->gst, j); };
+  auto res = [&]() { return spmv_pc(h, 1, x, b, h->V, nullptr, 0); };
+  return gmres_run<double>(h, K, x, h->opts.max_it, h->opts.rtol, h->opts.atol, h->opts.dtol, false, arn, res,
+                           its_out, reason_out);
+}
+
+// Mixed precision linear solve (4x4 blocks): FP64 iterative refinement around
+// FP32 GMRES cycles.  x64 = 0, r64 = b; per pass: b32 = r64/||r64||, one FP32
+// GMRES(m_inner) cycle with the FP32 point-block/Jacobi preconditioner to the
+// inner tolerance, x64 += ||r64|| * d, r64 = b - A32 x64 in FP64 arithmetic.
+// Stops when ||r64|| <= max(rtol*||b||, abs_target) or after max passes; the
+// Newton loop's FP64 residual then decides whether the step has converged.
+static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *passes_out,
+                       int *reason_out)
+{
+  const int64_t n = h->n;
+  int rc;
+  CK(cudaMemsetAsync(x, 0, sizeof(double) * n, h->stream));
+  CK(cudaMemcpyAsync(h->r64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+  double bnorm = 0.0;
+  if ((rc = norm2(h, b, &bnorm))) return rc;
+  const double target = std::max(h->opts.rtol * bnorm, h->abs_target);
+  int total = 0, passes = 0, reason = 2;
+  double rn = bnorm;
+  Krylov<float> K;
+  K.V = h->V32; K.m = h->m32; K.ldv = h->ldv; K.st = h->gst32; K.ga = h->ga32;
+  const int max_passes = 100;
+  while (rn > target && passes < max_passes && total < h->opts.max_it) {
+    // b32 = r64 / ||r64|| (the device norm lives in scalar[1])
+    if ((rc = norm2_dev(h, h->r64, h->scalar + 1))) return rc;
+    k_scale_to_f32<<<grid_for(n), 256, 0, h->stream>>>(n, h->r64, h->scalar + 1, h->b32);
+    pc_apply<4, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
+    h->launches += 2;
+    if ((rc = check_launch(h, "mixed_prepare"))) return rc;
+    auto arn = [&](int j) { return spmv32_pc(h, h->V32 + (int64_t)j * h->ldv, h->V32 + (int64_t)(j + 1) * h->ldv, h->gst32, j); };
+    auto nores = [&]() { return 0; };
+    int its = 0, r = 0;
+    if ((rc = gmres_run<float>(h, K, h->d64, h->m32, h->inner_rtol, 1e-50, 1e4, true, arn, nores, &its, &r)))
+      return rc;
+    total += its;
+    if (r == -9) { reason = -9; break; }    // NaN/Inf in the inner solve
+    // x += ||r|| d ; r = b - A32 x (FP64 accumulation)
+    k_axpy_dev<<<grid_for(n), 256, 0, h->stream>>>(n, h->scalar + 1, h->d64, x);
+    LAUNCHED(h);
+    {
+      const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 1, 8, 4, 0));
+      const int grid = (int)((h->nNode * 32LL + 255) / 256);
+      bsr4_spmv<1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b, nullptr,
+                                                           nullptr, h->r64, nullptr, 0);
+      prof_end(h, pi);
+      LAUNCHED(h);
+      if ((rc = check_launch(h, "mixed_residual"))) return rc;
+    }
+    passes++;
+    if ((rc = norm2(h, h->r64, &rn))) return rc;
+  }
+  if (rn > target) reason = (total >= h->opts.max_it) ? -3 : (reason < 0 ? reason : 0);
+  if (its_out) *its_out = total;
+  if (passes_out) *passes_out = passes;
+  if (reason_out) *reason_out = (rn <= target) ? 2 : reason;
+  return 0;
 }
 
 static int upload_td(cfdgpu_handle *h)
@@ -569,11 +703,41 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     CK(cudaMemset(*v, 0, sizeof(double) * n));
   }
   const size_t bb = (size_t)h->ndof * h->ndof;
-  if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
-  CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
-  if ((rc = dalloc(h, &h->dinv, (size_t)n))) return rc;
-  if ((rc = dalloc(h, &h->binv, (size_t)h->nNode * bb))) return rc;
+  h->mixed = (h->opts.precision == CFDGPU_PREC_MIXED);
+  if (h->mixed && h->ndof != 4) { h->err = "mixed precision is built for the 4x4-block (3D) systems"; return CFDGPU_EINVAL; }
   h->ldv = (n + 31) / 32 * 32;
+  if (h->mixed) {
+    // FP32 tangent and inner Krylov space; the FP64 matrix is not stored
+    h->m32 = (h->opts.inner_restart > 0) ? h->opts.inner_restart : 30;
+    if (h->m32 > 1000) { h->err = "inner restart > 1000 is not supported"; return CFDGPU_EINVAL; }
+    h->inner_rtol = (h->opts.inner_rtol > 0.0) ? h->opts.inner_rtol : 1e-4;
+    h->abs_target = 0.1 * h->ctrl.newton_tol;
+    h->m = 1;   // FP64 basis kept only as scratch for cfdgpu_true_residual
+    if ((rc = dalloc(h, &h->bsr32, (size_t)t.nnzb() * bb))) return rc;
+    CK(cudaMemset(h->bsr32, 0, sizeof(float) * t.nnzb() * bb));
+    if ((rc = dalloc(h, &h->dinv32, (size_t)n))) return rc;
+    if ((rc = dalloc(h, &h->binv32, (size_t)h->nNode * bb))) return rc;
+    if ((rc = dalloc(h, &h->V32, (size_t)h->ldv * (h->m32 + 1)))) return rc;
+    CK(cudaMemset(h->V32, 0, sizeof(float) * h->ldv * (h->m32 + 1)));
+    if ((rc = dalloc(h, &h->b32, (size_t)h->ldv))) return rc;
+    CK(cudaMemset(h->b32, 0, sizeof(float) * h->ldv));
+    if ((rc = dalloc(h, &h->r64, (size_t)n))) return rc;
+    if ((rc = dalloc(h, &h->d64, (size_t)n))) return rc;
+    if ((rc = dalloc(h, &h->gst32, 1))) return rc;
+    CK(cudaMemset(h->gst32, 0, sizeof(GmresState)));
+    if ((rc = dalloc(h, &h->ga32.H, (size_t)(h->m32 + 1) * h->m32))) return rc;
+    if ((rc = dalloc(h, &h->ga32.cs, (size_t)h->m32))) return rc;
+    if ((rc = dalloc(h, &h->ga32.sn, (size_t)h->m32))) return rc;
+    if ((rc = dalloc(h, &h->ga32.grs, (size_t)h->m32 + 1))) return rc;
+    if ((rc = dalloc(h, &h->ga32.y, (size_t)h->m32))) return rc;
+    const int64_t nt32 = (h->ldv / 4 + MAXPY_CHUNKS - 1) / MAXPY_CHUNKS;
+    if ((rc = dalloc(h, &h->ga32.partial, (size_t)(h->m32 + 1) * std::max<int64_t>(nt32, RED_BLOCKS)))) return rc;
+  } else {
+    if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
+    CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
+    if ((rc = dalloc(h, &h->dinv, (size_t)n))) return rc;
+    if ((rc = dalloc(h, &h->binv, (size_t)h->nNode * bb))) return rc;
+  }
   if ((rc = dalloc(h, &h->V, (size_t)h->ldv * (h->m + 1)))) return rc;
   CK(cudaMemset(h->V, 0, sizeof(double) * h->ldv * (h->m + 1)));
   if ((rc = dalloc(h, &h->gst, 1))) return rc;
@@ -583,7 +747,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   if ((rc = dalloc(h, &h->ga.grs, (size_t)h->m + 1))) return rc;
   if ((rc = dalloc(h, &h->ga.y, (size_t)h->m))) return rc;
   {
-    const int64_t ntiles = (h->ldv / 2 + MAXPY_PAIRS - 1) / MAXPY_PAIRS;
+    const int64_t ntiles = (h->ldv / 2 + MAXPY_CHUNKS - 1) / MAXPY_CHUNKS;
     if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
   }
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
@@ -658,10 +822,15 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     if (norm < h->ctrl.newton_tol) { stats->converged = 1; break; }
     auto ts = std::chrono::steady_clock::now();
     if (want_K && (rc = build_pc(h))) return rc;
-    int its = 0, reason = 0;
-    if ((rc = gmres(h, h->rhs, h->dx, &its, &reason))) return rc;
+    int its = 0, reason = 0, passes = 0;
+    if (h->mixed) {
+      if ((rc = solve_mixed(h, h->rhs, h->dx, &its, &passes, &reason))) return rc;
+    } else {
+      if ((rc = gmres(h, h->rhs, h->dx, &its, &reason))) return rc;
+    }
     stats->ksp_its[iter] = its;
     stats->ksp_reason[iter] = reason;
+    stats->refinements[iter] = passes;
     if (reason < 0) {
       h->err = "KSP diverged, reason " + std::to_string(reason) + " after " + std::to_string(its) + " iterations";
       return CFDGPU_EKSP;
@@ -807,6 +976,7 @@ int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int
 int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double *rhs)
 {
   if (!h) return CFDGPU_EINVAL;
+  if (h->mixed && bsr_vals) { h->err = "the FP64 matrix is not stored in mixed precision"; return CFDGPU_EINVAL; }
   if (!h->td_set) upload_td(h);
   int rc = assemble(h, iter, true);
   if (rc) return rc;
@@ -820,6 +990,7 @@ int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double 
 int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, int *reason)
 {
   if (!h || !b || !x) return CFDGPU_EINVAL;
+  if (h->mixed) { h->err = "cfdgpu_solve_export solves the FP64 system"; return CFDGPU_EINVAL; }
   if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
   CK(cudaMemcpyAsync(h->rhs, b, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
   int rc = build_pc(h);
@@ -837,6 +1008,7 @@ int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, 
 int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm)
 {
   if (!h || !x || !b || !norm) return CFDGPU_EINVAL;
+  if (h->mixed) { h->err = "cfdgpu_true_residual uses the FP64 matrix"; return CFDGPU_EINVAL; }
   if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
   // x -> dx, b -> rhs, r = b - A x -> applied-free scratch (the Krylov vector V_0)
   CK(cudaMemcpyAsync(h->dx, x, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
@@ -947,8 +1119,8 @@ extern "C" int cfdgpu_residual_norm_noalloc(int nNode, int ndof, const int32_t *
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned int), s) != cudaSuccess) return CFDGPU_ECUDA;
   if (ndof == 4) {
     const int grid = (int)((nNode * 32LL + 255) / 256);
-    bsr4_spmv_f64<1, 0><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr, nullptr, r,
-                                              nullptr, 0);
+    bsr4_spmv<1, 0, double><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr, nullptr, r,
+                                                nullptr, 0);
   } else {
     const int grid = (int)((n + 255) / 256);
     bsr_spmv_generic<3, 1, 0, double><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr,

@@ -94,15 +94,16 @@ __device__ __forceinline__ bool last_block(unsigned int *counter, unsigned int n
 }
 
 // ---------------------------------------------------------------------------
-// BSR SpMV, 4x4 FP64 blocks: one warp per block row; each lane loads 16 B of
-// a block (row q/2, columns 2(q%2), 2(q%2)+1 of block 'sub') so a warp
-// instruction reads four consecutive 128-B blocks.  MODE 0: y = M^-1 (A x),
-// MODE 1: y = M^-1 (b - A x).  PC: 0 none, 1 jacobi (dinv), 2 point-block
-// (binv, 4x4 per node, row-major).
-template <int MODE, int PC>
+// BSR SpMV, 4x4 blocks, FP64 vectors: one warp per block row; each lane loads
+// two entries of a block (row q/2, columns 2(q%2), 2(q%2)+1 of block 'sub'),
+// so a warp instruction reads four consecutive blocks (16-byte loads for FP64
+// blocks).  MT = float gives the FP64 residual of the FP32 matrix used by the
+// mixed-precision refinement.  MODE 0: y = M^-1 (A x), MODE 1: y = M^-1 (b - A x).
+// PC: 0 none, 1 jacobi (dinv), 2 point-block (binv, 4x4 per node, row-major).
+template <int MODE, int PC, typename MT>
 __global__ void __launch_bounds__(256)
-bsr4_spmv_f64(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
-              const double *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
+bsr4_spmv(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
+              const MT *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
               const double *__restrict__ dinv, const double *__restrict__ binv, double *__restrict__ y,
               const GmresState *__restrict__ st, int j)
 {
@@ -115,10 +116,17 @@ bsr4_spmv_f64(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__re
   double acc0 = 0.0, acc1 = 0.0;
   for (int kb = kb0 + sub; kb < kb1; kb += 4) {
     const int c = colidx[kb];
-    const double2 a = *reinterpret_cast<const double2 *>(val + (int64_t)kb * 16 + row * 4 + cp);
+    double a0, a1;
+    if constexpr (sizeof(MT) == 8) {
+      const double2 a = *reinterpret_cast<const double2 *>(val + (int64_t)kb * 16 + row * 4 + cp);
+      a0 = a.x; a1 = a.y;
+    } else {
+      const float2 a = *reinterpret_cast<const float2 *>(val + (int64_t)kb * 16 + row * 4 + cp);
+      a0 = a.x; a1 = a.y;
+    }
     const double2 xv = *reinterpret_cast<const double2 *>(x + (int64_t)c * 4 + cp);
-    acc0 = fma(a.x, xv.x, acc0);
-    acc0 = fma(a.y, xv.y, acc0);
+    acc0 = fma(a0, xv.x, acc0);
+    acc0 = fma(a1, xv.y, acc0);
   }
   double acc = acc0 + acc1;
   acc += __shfl_xor_sync(0xffffffffu, acc, 1);
@@ -137,6 +145,48 @@ bsr4_spmv_f64(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__re
     }
   } else if (lane < 8 && (lane & 1) == 0) {
     y[r] = (PC == 1) ? dinv[r] * v : v;
+  }
+}
+
+// BSR SpMV, 4x4 FP32 blocks and FP32 vectors (inner solve of the mixed
+// precision path): one warp per block row, lane = (block sub 0..7, row 0..3),
+// each lane loads one 16-byte block row and the matching 16 bytes of x, so a
+// warp instruction reads eight consecutive 64-byte blocks.
+template <int PC>
+__global__ void __launch_bounds__(256)
+bsr4_spmv_f32(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
+              const float *__restrict__ val, const float *__restrict__ x, const float *__restrict__ dinv,
+              const float *__restrict__ binv, float *__restrict__ y, const GmresState *__restrict__ st, int j)
+{
+  if (st && (!st->active || st->it != j)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nrows) return;
+  const int sub = lane >> 2, row = lane & 3;
+  const int kb0 = rowptr[warp], kb1 = rowptr[warp + 1];
+  float acc = 0.f;
+  for (int kb = kb0 + sub; kb < kb1; kb += 8) {
+    const int c = colidx[kb];
+    const float4 a = *reinterpret_cast<const float4 *>(val + (int64_t)kb * 16 + row * 4);
+    const float4 xv = *reinterpret_cast<const float4 *>(x + (int64_t)c * 4);
+    acc = fmaf(a.x, xv.x, acc);
+    acc = fmaf(a.y, xv.y, acc);
+    acc = fmaf(a.z, xv.z, acc);
+    acc = fmaf(a.w, xv.w, acc);
+  }
+  acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+  const int64_t r = (int64_t)warp * 4 + row;
+  if (PC == 2) {
+    const float v0 = __shfl_sync(0xffffffffu, acc, 0), v1 = __shfl_sync(0xffffffffu, acc, 1);
+    const float v2 = __shfl_sync(0xffffffffu, acc, 2), v3 = __shfl_sync(0xffffffffu, acc, 3);
+    if (lane < 4) {
+      const float *Bi = binv + (int64_t)warp * 16 + row * 4;
+      y[r] = Bi[0] * v0 + Bi[1] * v1 + Bi[2] * v2 + Bi[3] * v3;
+    }
+  } else if (lane < 4) {
+    y[r] = (PC == 1) ? dinv[r] * acc : acc;
   }
 }
 
@@ -185,9 +235,9 @@ __global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, 
 }
 
 // z = M^-1 r (stand-alone preconditioner application)
-template <int NB>
-__global__ void pc_apply(int64_t n, int pc, const double *__restrict__ dinv, const double *__restrict__ binv,
-                         const double *__restrict__ r, double *__restrict__ z)
+template <int NB, typename VT, typename PT>
+__global__ void pc_apply(int64_t n, int pc, const PT *__restrict__ dinv, const PT *__restrict__ binv,
+                         const VT *__restrict__ r, VT *__restrict__ z)
 {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -196,19 +246,19 @@ __global__ void pc_apply(int64_t n, int pc, const double *__restrict__ dinv, con
     const int row = (int)(t % NB);
     double s = 0.0;
 #pragma unroll
-    for (int q = 0; q < NB; q++) s += binv[node * NB * NB + row * NB + q] * r[node * NB + q];
-    z[t] = s;
+    for (int q = 0; q < NB; q++) s += (double)binv[node * NB * NB + row * NB + q] * (double)r[node * NB + q];
+    z[t] = (VT)s;
   } else if (pc == 1) {
-    z[t] = dinv[t] * r[t];
+    z[t] = (VT)((double)dinv[t] * (double)r[t]);
   } else {
     z[t] = r[t];
   }
 }
 
 // Scalar-diagonal inverse and point-block inverses of the assembled matrix.
-template <int NB, typename VT>
+template <int NB, typename VT, typename PT>
 __global__ void build_jacobi(int nnode, const int32_t *__restrict__ diag_slot, const VT *__restrict__ val,
-                             double *__restrict__ dinv, double *__restrict__ binv, int pc)
+                             PT *__restrict__ dinv, PT *__restrict__ binv, int pc)
 {
   const int node = blockIdx.x * blockDim.x + threadIdx.x;
   if (node >= nnode) return;
@@ -217,7 +267,7 @@ __global__ void build_jacobi(int nnode, const int32_t *__restrict__ diag_slot, c
 #pragma unroll
     for (int a = 0; a < NB; a++) {
       const double d = (double)B[a * NB + a];
-      dinv[(int64_t)node * NB + a] = (d != 0.0) ? 1.0 / d : 1.0;
+      dinv[(int64_t)node * NB + a] = (PT)((d != 0.0) ? 1.0 / d : 1.0);
     }
     return;
   }
@@ -255,7 +305,7 @@ __global__ void build_jacobi(int nnode, const int32_t *__restrict__ diag_slot, c
 #pragma unroll
   for (int a = 0; a < NB; a++)
 #pragma unroll
-    for (int c = 0; c < NB; c++) binv[(int64_t)node * NB * NB + a * NB + c] = I[a][c];
+    for (int c = 0; c < NB; c++) binv[(int64_t)node * NB * NB + a * NB + c] = (PT)I[a][c];
 }
 
 // ---------------------------------------------------------------------------
@@ -279,14 +329,45 @@ norm2_kernel(int64_t n, const double *__restrict__ x, double *__restrict__ parti
   }
 }
 
+// 16-byte chunks of a Krylov vector: 2 doubles or 4 floats.  Arithmetic on
+// the values is FP64 in every kernel; FP32 vectors only change the storage.
+template <typename VT> struct Chunk;
+template <> struct Chunk<double> {
+  static constexpr int E = 2;
+  static __device__ __forceinline__ void load(const double *p, double (&v)[2])
+  {
+    const double2 t = *reinterpret_cast<const double2 *>(p);
+    v[0] = t.x; v[1] = t.y;
+  }
+  static __device__ __forceinline__ void store(double *p, const double (&v)[2])
+  {
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  }
+};
+template <> struct Chunk<float> {
+  static constexpr int E = 4;
+  static __device__ __forceinline__ void load(const float *p, double (&v)[4])
+  {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  }
+  static __device__ __forceinline__ void store(float *p, const double (&v)[4])
+  {
+    *reinterpret_cast<float4 *>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+  }
+};
+
 // GMRES cycle start: res = ||V0||, convergence test at its, v0scale.
+template <typename VT>
 __global__ void __launch_bounds__(RED_THREADS)
-gmres_start(int64_t n, const double *__restrict__ v0, GmresState *st, GmresArrays ga)
+gmres_start(int64_t n, const VT *__restrict__ v0, GmresState *st, GmresArrays ga)
 {
   __shared__ double sh[RED_THREADS / 32];
   double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS)
-    s = fma(v0[i], v0[i], s);
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
+    const double v = (double)v0[i];
+    s = fma(v, v, s);
+  }
   s = block_sum<RED_THREADS>(s, sh);
   if (threadIdx.x == 0) ga.partial[blockIdx.x] = s;
   if (last_block(&st->counter, gridDim.x)) {
@@ -310,47 +391,53 @@ gmres_start(int64_t n, const double *__restrict__ v0, GmresState *st, GmresArray
   }
 }
 
-__global__ void scale_v0(int64_t n, double *__restrict__ v0, const GmresState *__restrict__ st)
+template <typename VT>
+__global__ void scale_v0(int64_t n, VT *__restrict__ v0, const GmresState *__restrict__ st)
 {
   const double s = st->v0scale;
   if (s == 0.0) return;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v0[i] *= s;
+    v0[i] = (VT)((double)v0[i] * s);
 }
 
 // Hessenberg storage: column-major, leading dimension m+1: H(r, c) = H[c*(m+1) + r].
 __device__ __forceinline__ int64_t hidx(int r, int c, int m) { return (int64_t)c * (m + 1) + r; }
 
 // Krylov vectors are stored with a leading dimension ldv that is a multiple
-// of 32 doubles; entries n..ldv-1 stay zero, so every kernel below processes
-// pairs of doubles (16-byte loads) over npair = ldv/2.
+// of 32 entries; entries n..ldv-1 stay zero, so every kernel below processes
+// 16-byte chunks (Chunk<VT>::E entries) over nchunk = ldv / E.
 constexpr int ORTHO_THREADS = 256;
 constexpr int MDOT_KC = 8;          // basis vectors per CTA in the multi-dot
 
-__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
-
 // Classical Gram-Schmidt dot products, pass 1: per column tile partial sums
 // of <w, V_k> for a chunk of MDOT_KC vectors.  grid (ntiles, ceil((j+1)/KC)).
+template <typename VT>
 __global__ void __launch_bounds__(ORTHO_THREADS)
-gmres_mdot(int64_t npair, const double *__restrict__ V, int64_t ldv, int j, const GmresState *__restrict__ st,
+gmres_mdot(int64_t nchunk, const VT *__restrict__ V, int64_t ldv, int j, const GmresState *__restrict__ st,
            double *__restrict__ partial)
 {
   if (!st->active || st->it != j) return;
+  constexpr int E = Chunk<VT>::E;
   __shared__ double sh[MDOT_KC][ORTHO_THREADS / 32];
   const int k0 = blockIdx.y * MDOT_KC;
   const int nk = min(MDOT_KC, j + 1 - k0);
   const int64_t p = (int64_t)blockIdx.x * ORTHO_THREADS + threadIdx.x;
-  const double *w = V + (int64_t)(j + 1) * ldv;
+  const VT *w = V + (int64_t)(j + 1) * ldv;
   double acc[MDOT_KC];
 #pragma unroll
   for (int q = 0; q < MDOT_KC; q++) acc[q] = 0.0;
-  if (p < npair) {
-    const double2 wv = ld2(w + 2 * p);
+  if (p < nchunk) {
+    double wv[E];
+    Chunk<VT>::load(w + E * p, wv);
 #pragma unroll
     for (int q = 0; q < MDOT_KC; q++) {
       if (q < nk) {
-        const double2 v = ld2(V + (int64_t)(k0 + q) * ldv + 2 * p);
-        acc[q] = fma(wv.x, v.x, wv.y * v.y);
+        double v[E];
+        Chunk<VT>::load(V + (int64_t)(k0 + q) * ldv + E * p, v);
+        double a = wv[0] * v[0];
+#pragma unroll
+        for (int e = 1; e < E; e++) a = fma(wv[e], v[e], a);
+        acc[q] = a;
       }
     }
   }
@@ -387,57 +474,72 @@ __global__ void gmres_mdot_reduce(int ntiles, int j, const GmresState *__restric
   if (lane == 0) H[hidx(k, j, st->m)] = t;
 }
 
-// w -= sum_k H(k, j) V_k, then ||w||^2 partials.  A CTA covers MAXPY_PAIRS
-// column pairs; its four thread quarters take the k's congruent to 0..3 mod 4
-// (16-byte loads, consecutive lanes on consecutive pairs), and the quarter
-// sums are combined in a fixed order through shared memory.  The last CTA
-// finishes the norm, applies the stored Givens rotations to column j, forms
-// the new one and runs the convergence test (KSPGMRESUpdateHessenberg,
-// KSPConvergedDefault).
-constexpr int MAXPY_PAIRS = 64;
+// w -= sum_k H(k, j) V_k, then ||w||^2 partials.  A CTA covers MAXPY_CHUNKS
+// 16-byte chunks; its four thread quarters take the k's congruent to 0..3
+// mod 4 (consecutive lanes on consecutive chunks), and the quarter sums are
+// combined in a fixed order through shared memory.  The last CTA finishes the
+// norm, applies the stored Givens rotations to column j, forms the new one and
+// runs the convergence test (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
+constexpr int MAXPY_CHUNKS = 64;
+template <typename VT>
 __global__ void __launch_bounds__(ORTHO_THREADS)
-gmres_maxpy_norm(int64_t npair, double *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
+gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
 {
   if (!st->active || st->it != j) return;
+  constexpr int E = Chunk<VT>::E;
   __shared__ double hk[1024];
   __shared__ double sh[ORTHO_THREADS / 32];
-  __shared__ double2 qs[ORTHO_THREADS / MAXPY_PAIRS][MAXPY_PAIRS];
+  __shared__ double qs[ORTHO_THREADS / MAXPY_CHUNKS][E][MAXPY_CHUNKS];
   const int m = st->m;
   for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[hidx(k, j, m)];
   __syncthreads();
-  double *w = V + (int64_t)(j + 1) * ldv;
-  const int lp = threadIdx.x % MAXPY_PAIRS;
-  const int quarter = threadIdx.x / MAXPY_PAIRS;
-  const int64_t p = (int64_t)blockIdx.x * MAXPY_PAIRS + lp;
-  double2 acc = make_double2(0.0, 0.0);
-  if (p < npair) {
-    const double *base = V + 2 * p;
+  VT *w = V + (int64_t)(j + 1) * ldv;
+  const int lp = threadIdx.x % MAXPY_CHUNKS;
+  const int quarter = threadIdx.x / MAXPY_CHUNKS;
+  const int64_t p = (int64_t)blockIdx.x * MAXPY_CHUNKS + lp;
+  double acc[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) acc[e] = 0.0;
+  if (p < nchunk) {
+    const VT *base = V + E * p;
     int k = quarter;
     for (; k + 12 <= j; k += 16) {
-      const double2 v0 = ld2(base + (int64_t)k * ldv);
-      const double2 v1 = ld2(base + (int64_t)(k + 4) * ldv);
-      const double2 v2 = ld2(base + (int64_t)(k + 8) * ldv);
-      const double2 v3 = ld2(base + (int64_t)(k + 12) * ldv);
-      acc.x = fma(hk[k], v0.x, acc.x); acc.y = fma(hk[k], v0.y, acc.y);
-      acc.x = fma(hk[k + 4], v1.x, acc.x); acc.y = fma(hk[k + 4], v1.y, acc.y);
-      acc.x = fma(hk[k + 8], v2.x, acc.x); acc.y = fma(hk[k + 8], v2.y, acc.y);
-      acc.x = fma(hk[k + 12], v3.x, acc.x); acc.y = fma(hk[k + 12], v3.y, acc.y);
+      double v0[E], v1[E], v2[E], v3[E];
+      Chunk<VT>::load(base + (int64_t)k * ldv, v0);
+      Chunk<VT>::load(base + (int64_t)(k + 4) * ldv, v1);
+      Chunk<VT>::load(base + (int64_t)(k + 8) * ldv, v2);
+      Chunk<VT>::load(base + (int64_t)(k + 12) * ldv, v3);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        acc[e] = fma(hk[k], v0[e], acc[e]);
+        acc[e] = fma(hk[k + 4], v1[e], acc[e]);
+        acc[e] = fma(hk[k + 8], v2[e], acc[e]);
+        acc[e] = fma(hk[k + 12], v3[e], acc[e]);
+      }
     }
     for (; k <= j; k += 4) {
-      const double2 v0 = ld2(base + (int64_t)k * ldv);
-      acc.x = fma(hk[k], v0.x, acc.x); acc.y = fma(hk[k], v0.y, acc.y);
+      double v0[E];
+      Chunk<VT>::load(base + (int64_t)k * ldv, v0);
+#pragma unroll
+      for (int e = 0; e < E; e++) acc[e] = fma(hk[k], v0[e], acc[e]);
     }
   }
-  qs[quarter][lp] = acc;
+#pragma unroll
+  for (int e = 0; e < E; e++) qs[quarter][e][lp] = acc[e];
   __syncthreads();
   double s = 0.0;
-  if (quarter == 0 && p < npair) {
-    double2 a = ld2(w + 2 * p);
-    const double2 q0 = qs[0][lp], q1 = qs[1][lp], q2 = qs[2][lp], q3 = qs[3][lp];
-    a.x -= ((q0.x + q1.x) + (q2.x + q3.x));
-    a.y -= ((q0.y + q1.y) + (q2.y + q3.y));
-    *reinterpret_cast<double2 *>(w + 2 * p) = a;
-    s = fma(a.x, a.x, a.y * a.y);
+  if (quarter == 0 && p < nchunk) {
+    double a[E];
+    Chunk<VT>::load(w + E * p, a);
+#pragma unroll
+    for (int e = 0; e < E; e++) a[e] -= ((qs[0][e][lp] + qs[1][e][lp]) + (qs[2][e][lp] + qs[3][e][lp]));
+    Chunk<VT>::store(w + E * p, a);
+    // the norm is taken of the stored (possibly rounded) values
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const double v = (double)(VT)a[e];
+      s = fma(v, v, s);
+    }
   }
   s = block_sum<ORTHO_THREADS>(s, sh);
   if (threadIdx.x == 0) ga.partial[blockIdx.x] = s;
@@ -505,18 +607,22 @@ gmres_maxpy_norm(int64_t npair, double *__restrict__ V, int64_t ldv, int j, Gmre
 }
 
 // V_{j+1} /= tt (VecNormalize), only if step j ran
-__global__ void gmres_scale_next(int64_t npair, double *__restrict__ V, int64_t ldv, int j,
+template <typename VT>
+__global__ void gmres_scale_next(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j,
                                  const GmresState *__restrict__ st)
 {
   if (st->it != j + 1) return;
   const double tt = st->tt;
   if (tt == 0.0) return;
+  constexpr int E = Chunk<VT>::E;
   const double s = 1.0 / tt;
-  double *w = V + (int64_t)(j + 1) * ldv;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npair; p += (int64_t)gridDim.x * blockDim.x) {
-    double2 a = ld2(w + 2 * p);
-    a.x *= s; a.y *= s;
-    *reinterpret_cast<double2 *>(w + 2 * p) = a;
+  VT *w = V + (int64_t)(j + 1) * ldv;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nchunk; p += (int64_t)gridDim.x * blockDim.x) {
+    double a[E];
+    Chunk<VT>::load(w + E * p, a);
+#pragma unroll
+    for (int e = 0; e < E; e++) a[e] *= s;
+    Chunk<VT>::store(w + E * p, a);
   }
 }
 
@@ -544,10 +650,11 @@ __global__ void __launch_bounds__(1024) gmres_backsub(GmresState *st, GmresArray
   }
 }
 
-// x += sum_{k < it} y_k V_k
+// x += scale * sum_{k < it} y_k V_k  (x is FP64 whatever the basis type)
+template <typename VT>
 __global__ void __launch_bounds__(ORTHO_THREADS)
-gmres_update_x(int64_t n, double *__restrict__ x, const double *__restrict__ V, int64_t ldv,
-               const GmresState *__restrict__ st, GmresArrays ga)
+gmres_update_x(int64_t n, double *__restrict__ x, const VT *__restrict__ V, int64_t ldv,
+               const GmresState *__restrict__ st, GmresArrays ga, double scale)
 {
   __shared__ double yk[1024];
   const int it = st->it;
@@ -556,9 +663,26 @@ gmres_update_x(int64_t n, double *__restrict__ x, const double *__restrict__ V, 
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int k = 0; k < it; k++) s = fma(yk[k], V[(int64_t)k * ldv + i], s);
-    x[i] += s;
+    for (int k = 0; k < it; k++) s = fma(yk[k], (double)V[(int64_t)k * ldv + i], s);
+    x[i] += scale * s;
   }
+}
+
+// mixed precision helpers: b32 = r64 * s (FP32), x64 += a * d64
+__global__ void k_scale_to_f32(int64_t n, const double *__restrict__ r, const double *__restrict__ norm,
+                               float *__restrict__ b32)
+{
+  const double s = (norm[0] != 0.0) ? 1.0 / norm[0] : 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b32[i] = (float)(r[i] * s);
+}
+
+__global__ void k_axpy_dev(int64_t n, const double *__restrict__ a, const double *__restrict__ d,
+                           double *__restrict__ x)
+{
+  const double s = a[0];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += s * d[i];
 }
 
 __global__ void gmres_init(GmresState *st, int m, int maxit, double rtol, double atol, double dtol)
