@@ -12,7 +12,7 @@ file carries PETSc option names:
 plus this library's own keys:
 
   -gpu_precision fp64|mixed   -gpu_inner_restart m    -gpu_inner_rtol r
-  -gpu_reuse_tangent 0|1
+  -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_newton_rtol r
 
 The GPU library has no direct solver.  ``-ksp_type preonly -pc_type lu`` (the
 reference's shipped tests) is served by GMRES with point-block Jacobi at a
@@ -69,6 +69,10 @@ def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
         kw["inner_rtol"] = float(opts["-gpu_inner_rtol"])
     if "-gpu_reuse_tangent" in opts:
         kw["reuse_tangent"] = bool(int(opts["-gpu_reuse_tangent"]))
+    if "-gpu_refine_rtol" in opts:
+        kw["refine_rtol"] = float(opts["-gpu_refine_rtol"])
+    if "-gpu_newton_rtol" in opts:
+        kw["newton_rtol"] = float(opts["-gpu_newton_rtol"])
     kw["_notes"] = notes
     return kw
 

@@ -94,6 +94,8 @@ typedef struct cfdgpu_solver_opts {
   int inner_restart;        /* mixed mode: FP32 inner GMRES restart (0: = restart) */
   double inner_rtol;        /* mixed mode: inner relative tolerance per refinement pass */
   int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
+  double refine_rtol;       /* mixed mode: FP64 refinement target ||b - A32 x|| <= refine_rtol ||b|| per Newton solve */
+  double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0|| (0: off, the reference's test only) */
 } cfdgpu_solver_opts;
 
 #define CFDGPU_MAX_NEWTON 32
