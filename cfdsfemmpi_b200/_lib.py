@@ -173,8 +173,8 @@ class Handle:
 
     def __init__(self, mesh, ctrl, restart: int = 50, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e4,
                  max_it: int = 10000, pc: str = "jacobi", precision: str = "fp64", inner_restart: int = 0,
-                 inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
-                 newton_max_iter: int = 10, refine_rtol: float = 1e-6, newton_rtol: Optional[float] = None):
+                 inner_rtol: float = 1e-6, reuse_tangent: bool = True, newton_tol: float = 1e-8,
+                 newton_max_iter: int = 10, refine_rtol: float = 1e-12, newton_rtol: float = 0.0):
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()
@@ -184,8 +184,6 @@ class Handle:
         m, self._keep = _mesh_struct(mesh)
         c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
                     ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
-        if newton_rtol is None:
-            newton_rtol = 1e-10 if precision == "mixed" else 0.0
         o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
                        1 if reuse_tangent else 0, refine_rtol, newton_rtol)
         rc = L.cfdgpu_create(ctypes.byref(m), ctypes.byref(c), ctypes.byref(o), ctypes.byref(self.h))
