@@ -55,21 +55,28 @@ def parse():
     p.add_argument("--workload", default="ldc3d_32", choices=list(WORKLOADS))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                   help="mixed: FP32 tangent storage and FP32 inner GMRES(100) with FP64 refinement")
     return p.parse_args()
 
 
-def make_case(name):
+def make_case(name, precision="fp64"):
     from cfdsfemmpi_b200 import meshgen
     n, steps, opts = WORKLOADS[name]
     mesh, ctrl, _ = meshgen.case_hex(n, steps, mu=0.001, dt=0.1)
-    return mesh, ctrl, dict(opts)
+    opts = dict(opts)
+    if precision == "mixed":
+        opts.update(precision="mixed", inner_restart=100, inner_rtol=1e-4, max_it=40000)
+    return mesh, ctrl, opts
 
 
 def workload_config(name, mesh, opts, extra=None):
     n = WORKLOADS[name][0]
     cfg = {"workload": f"{name}: graded-cube lid-driven cavity, {n}^3 hex8 ({mesh.nElem} elements, "
                        f"{mesh.nNode} nodes, {mesh.nNode * 4} dofs), Re 1000, dt 0.1, gen-alpha rho_inf 0",
-           "method": "plain (reference-identical constant predictor), FP64",
+           "method": ("plain (reference-identical constant predictor), FP64" if opts.get("precision", "fp64") == "fp64"
+                      else "plain predictor, mixed precision: FP32 tangent + FP32 GMRES(100) cycles, FP64 refinement "
+                           "and FP64 Newton residual"),
            "solver": f"Newton to 1e-8 abs; GMRES({opts['restart']}) + {opts['pc']}, rtol {opts['rtol']:g}",
            "l2": "flushed between timed steps (256 MiB write)"}
     if extra:
@@ -151,7 +158,7 @@ def run_ours(args, world, rank, local):
     from cfdsfemmpi_b200 import Handle
 
     torch.cuda.set_device(local)
-    mesh, ctrl, opts = make_case(args.workload)
+    mesh, ctrl, opts = make_case(args.workload, args.precision)
     h = Handle(mesh, ctrl, **opts)
     stream = torch.cuda.ExternalStream(h.stream_ptr())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -263,7 +270,7 @@ def run_ours(args, world, rank, local):
     newt = [s["newton_iters"] for s in stats]
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic: graded-cube hex8 cavity generated in-process (no dataset)",
             "config": workload_config(args.workload, mesh, opts,
                                       {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",

@@ -173,8 +173,8 @@ class Handle:
 
     def __init__(self, mesh, ctrl, restart: int = 50, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e4,
                  max_it: int = 10000, pc: str = "jacobi", precision: str = "fp64", inner_restart: int = 0,
-                 inner_rtol: float = 1e-6, reuse_tangent: bool = True, newton_tol: float = 1e-8,
-                 newton_max_iter: int = 10, refine_rtol: float = 1e-12, newton_rtol: float = 0.0):
+                 inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
+                 newton_max_iter: int = 10, refine_rtol: float = 1e-10, newton_rtol: float = 0.0):
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()

@@ -314,9 +314,16 @@ static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, doub
   ElemParams P;
   P.rho = h->ctrl.rho; P.mu = h->ctrl.mu; P.af = h->td[2]; P.am = h->td[1]; P.acceFact = h->td[8];
   P.stab0 = h->ctrl.stab[0]; P.stab1 = h->ctrl.stab[1]; P.stab2 = h->ctrl.stab[2];
-  element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
-      elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
-      h->rhs, outK, outF, h->negjac);
+  if (h->mixed && MODE != MODE_EXPORT) {
+    // FP64 arithmetic, FP32 storage of the tangent blocks
+    element_kernel<ET, double, float, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+        elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr32,
+        h->rhs, outK, outF, h->negjac);
+  } else {
+    element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+        elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
+        h->rhs, outK, outF, h->negjac);
+  }
   prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "element_kernel");
@@ -354,20 +361,16 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
   }
   if (want_K && !t.fixed_dofs.empty()) {
     const int nfix = (int)t.fixed_dofs.size();
-    k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
+    if (h->mixed)
+      k_dirichlet_diag<float><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr32);
+    else
+      k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
     LAUNCHED(h);
     int rc = check_launch(h, "dirichlet_diag");
     if (rc) return rc;
     h->assembled_K = true;
   }
-  if (want_K && h->mixed) {
-    // FP32 copy of the tangent for the inner solves
-    const int64_t nv = h->topo.nnzb() * h->ndof * h->ndof;
-    k_round_f32<<<grid_for(nv / 4), 256, 0, h->stream>>>(nv / 4, h->bsr, h->bsr32);
-    LAUNCHED(h);
-    int rc = check_launch(h, "round_f32");
-    if (rc) return rc;
-  }
+
   return 0;
 }
 
@@ -377,7 +380,7 @@ static int build_pc(cfdgpu_handle *h)
   if (pc == CFDGPU_PC_NONE) return 0;
   const int g = (h->nNode + 127) / 128;
   if (h->mixed) {
-    build_jacobi<4, double, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv32, h->binv32, pc);
+    build_jacobi<4, float, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr32, h->dinv32, h->binv32, pc);
   } else if (h->ndof == 4) {
     build_jacobi<4, double, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
   } else {
@@ -566,12 +569,13 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
 
 // Mixed precision linear solve (4x4 blocks): FP64 iterative refinement around
 // FP32 GMRES cycles.  x64 = 0, r64 = b; per pass: b32 = r64/||r64||, one FP32
-// GMRES(m_inner) cycle (FP32 matrix copy, FP32 Krylov basis, FP32
-// preconditioner; FP64 dot products and Hessenberg) to the inner tolerance,
-// x64 += ||r64|| * d, r64 = b - A x64 with the FP64 matrix.
-// Stops when ||r64|| <= refine_rtol*||b|| or after max passes.  Because the
-// refinement residual uses the FP64 tangent, the answer is the FP64 system's;
-// FP32 only changes how many inner iterations it takes.
+// GMRES(m_inner) cycle (FP32 matrix, FP32 Krylov basis, FP32 preconditioner;
+// FP64 dot products and Hessenberg) to the inner tolerance,
+// x64 += ||r64|| * d, r64 = b - A32 x64 accumulated in FP64.
+// Stops when ||r64|| <= max(refine_rtol*||b||, 0.1*newton_tol) or after max
+// passes: the linear solve is not carried below the nonlinear tolerance, and
+// the Newton loop's FP64 residual (element kernels in FP64) decides whether
+// the step has converged and corrects the FP32 rounding of the tangent.
 static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *passes_out,
                        int *reason_out)
 {
@@ -581,7 +585,7 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
   CK(cudaMemcpyAsync(h->r64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
   double bnorm = 0.0;
   if ((rc = norm2(h, b, &bnorm))) return rc;
-  const double target = std::max(h->refine_rtol * bnorm, 1e-300);
+  const double target = std::max(h->refine_rtol * bnorm, 0.1 * h->ctrl.newton_tol);
   int total = 0, passes = 0, reason = 2;
   double rn = bnorm;
   Krylov<float> K;
@@ -605,10 +609,10 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
     k_axpy_dev<<<grid_for(n), 256, 0, h->stream>>>(n, h->scalar + 1, h->d64, x);
     LAUNCHED(h);
     {
-      const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 1, 8, 8, 0));
+      const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 1, 8, 4, 0));
       const int grid = (int)((h->nNode * 32LL + 255) / 256);
-      bsr4_spmv<1, 0, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, nullptr,
-                                                            nullptr, h->r64, nullptr, 0);
+      bsr4_spmv<1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b, nullptr,
+                                                           nullptr, h->r64, nullptr, 0);
       prof_end(h, pi);
       LAUNCHED(h);
       if ((rc = check_launch(h, "mixed_residual"))) return rc;
@@ -718,14 +722,12 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   if (h->mixed && h->ndof != 4) { h->err = "mixed precision is built for the 4x4-block (3D) systems"; return CFDGPU_EINVAL; }
   h->ldv = (n + 31) / 32 * 32;
   if (h->mixed) {
-    // FP32 copy of the tangent and FP32 inner Krylov space next to the FP64 matrix
-    h->m32 = (h->opts.inner_restart > 0) ? h->opts.inner_restart : h->opts.restart;
+    // FP32 tangent and FP32 inner Krylov space; the FP64 matrix is not stored
+    h->m32 = (h->opts.inner_restart > 0) ? h->opts.inner_restart : 100;
     if (h->m32 > 1000) { h->err = "inner restart > 1000 is not supported"; return CFDGPU_EINVAL; }
-    h->inner_rtol = (h->opts.inner_rtol > 0.0) ? h->opts.inner_rtol : 1e-6;
-    h->refine_rtol = (h->opts.refine_rtol > 0.0) ? h->opts.refine_rtol : 1e-12;
-    h->m = 1;   // FP64 basis kept only as scratch for cfdgpu_true_residual
-    if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
-    CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
+    h->inner_rtol = (h->opts.inner_rtol > 0.0) ? h->opts.inner_rtol : 1e-4;
+    h->refine_rtol = (h->opts.refine_rtol > 0.0) ? h->opts.refine_rtol : 1e-10;
+    h->m = 1;   // FP64 basis kept only as scratch
     if ((rc = dalloc(h, &h->bsr32, (size_t)t.nnzb() * bb))) return rc;
     CK(cudaMemset(h->bsr32, 0, sizeof(float) * t.nnzb() * bb));
     if ((rc = dalloc(h, &h->dinv32, (size_t)n))) return rc;
@@ -994,6 +996,7 @@ int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int
 int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double *rhs)
 {
   if (!h) return CFDGPU_EINVAL;
+  if (h->mixed && bsr_vals) { h->err = "the FP64 matrix is not stored in mixed precision"; return CFDGPU_EINVAL; }
 
   if (!h->td_set) upload_td(h);
   int rc = assemble(h, iter, true);
@@ -1026,6 +1029,7 @@ int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, 
 int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm)
 {
   if (!h || !x || !b || !norm) return CFDGPU_EINVAL;
+  if (h->mixed) { h->err = "cfdgpu_true_residual uses the FP64 matrix"; return CFDGPU_EINVAL; }
 
   if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
   // x -> dx, b -> rhs, r = b - A x -> applied-free scratch (the Krylov vector V_0)

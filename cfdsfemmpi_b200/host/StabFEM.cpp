@@ -141,7 +141,7 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
   const std::string ksp = get("-ksp_type", "gmres"), pc = get("-pc_type", "");
   opts_.restart = 30; opts_.rtol = 1e-5; opts_.atol = 1e-50; opts_.dtol = 1e4; opts_.max_it = 10000;
   opts_.pc_type = CFDGPU_PC_PBJACOBI; opts_.precision = CFDGPU_PREC_FP64; opts_.inner_restart = 0;
-  opts_.inner_rtol = 1e-4; opts_.reuse_tangent = 1; opts_.refine_rtol = 1e-12; opts_.newton_rtol = 0.0;
+  opts_.inner_rtol = 1e-4; opts_.reuse_tangent = 1; opts_.refine_rtol = 1e-10; opts_.newton_rtol = 0.0;
   const bool direct = (ksp == "preonly" || pc == "lu" || pc == "cholesky");
   if (direct) {
     // no direct solver on the GPU: tight GMRES + point-block Jacobi substitutes

@@ -52,7 +52,7 @@ extern "C" {
 
 /* precision modes */
 #define CFDGPU_PREC_FP64 0      /* FP64 element kernels, matrix and Krylov solve */
-#define CFDGPU_PREC_MIXED 1     /* FP32 matrix copy + FP32 inner GMRES, FP64 tangent/residual/refinement */
+#define CFDGPU_PREC_MIXED 1     /* FP32 tangent storage + FP32 inner GMRES, FP64 residual/refinement */
 
 /* Mesh: borrowed host arrays, copied at create (StabFEM::readInputData,
  * StabFEM.cpp:80-264).  conn is 0-based, nElem*npElem; DBC entries are
@@ -91,10 +91,10 @@ typedef struct cfdgpu_solver_opts {
   int max_it;
   int pc_type;
   int precision;            /* CFDGPU_PREC_* */
-  int inner_restart;        /* mixed mode: FP32 inner GMRES restart (0: = restart) */
-  double inner_rtol;        /* mixed mode: inner relative tolerance per refinement pass (0: 1e-6) */
+  int inner_restart;        /* mixed mode: FP32 inner GMRES restart (0: 100) */
+  double inner_rtol;        /* mixed mode: inner relative tolerance per refinement pass (0: 1e-4) */
   int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
-  double refine_rtol;       /* mixed mode: FP64 refinement target ||b - A x|| <= refine_rtol ||b|| per solve (0: 1e-12) */
+  double refine_rtol;       /* mixed mode: refinement target ||b - A32 x|| <= max(refine_rtol ||b||, newton_tol/10) (0: 1e-10) */
   double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0|| (0: off, the reference's test only) */
 } cfdgpu_solver_opts;
 
