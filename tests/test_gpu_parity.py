@@ -276,3 +276,65 @@ def test_mixed_precision_path(n, steps):
     assert all(s["norms"][-1] < 1e-8 for s in st_mix)
     rel = np.linalg.norm(mix - ref) / np.linalg.norm(ref)
     assert rel < 5e-2, rel
+
+
+@pytest.mark.parametrize("kind", list(MESHES))
+def test_gpu_tangent_matches_finite_difference(kind):
+    """diffStiffTest analogue (src/base/StabFEM.cpp:581-706) on the GPU element
+    kernels: K from cfdgpu_element_matrices equals -dF/dsoln by central
+    differences of F through the generalised-alpha chain (solnCur, solnDotCur)."""
+    mesh = MESHES[kind]()
+    ctrl = meshgen.control_for(5, 0.1, 0.01, tis=2)
+    td = oracle.time_params(2, 0.0, 0.1)
+    n = mesh.nNode * mesh.ndof
+    rng = np.random.default_rng(21)
+    prev = 0.3 * rng.standard_normal(n)
+    dotprev = 0.1 * rng.standard_normal(n)
+    soln = 0.3 * rng.standard_normal(n)
+    h = Handle(mesh, ctrl)
+
+    def KF(s):
+        cur = td[2] * s + (1 - td[2]) * prev
+        dot = td[9] * s + td[10] * prev + td[15] * dotprev
+        dotcur = td[1] * dot + (1 - td[1]) * dotprev
+        h.set_element_state(prev, cur, dotcur)
+        return h.element_matrices(np.array([0], np.int32))
+
+    K, _ = KF(soln)
+    nodes = mesh.conn[0]
+    ndof = mesh.ndof
+    g = (nodes[:, None] * ndof + np.arange(ndof)).ravel()
+    eps = 1e-6
+    Kfd = np.zeros_like(K[0])
+    for j, gj in enumerate(g):
+        sp = soln.copy(); sm = soln.copy()
+        sp[gj] += eps; sm[gj] -= eps
+        Kfd[:, j] = -(KF(sp)[1][0] - KF(sm)[1][0]) / (2 * eps)
+    h.close()
+    assert np.abs(K[0] - Kfd).max() / np.abs(K[0]).max() < 1e-7
+
+
+def test_vtu_and_forces_output(golden_dir, tmp_path):
+    """StabFEM.postProcess writes <prefix>-%06d.vtu per step with velocity (3
+    components), pressure and procId; the forces file gets one line per step."""
+    import shutil
+    from cfdsfemmpi_b200.vtu import read_vtu_point_data
+    src = os.path.join(golden_dir, "ldc2dquad10")
+    for f in os.listdir(src):
+        shutil.copy(os.path.join(src, f), tmp_path / f)
+    fem = StabFEM()
+    fem.readInputData(str(tmp_path / "LDC2Dquad10"))
+    fem.readControlParameters(str(tmp_path / "control-parameters-ldc-Re100.dat"))
+    fem.write_vtu = True
+    fem.setSolver(1, None, False, options={"-ksp_type": "gmres", "-ksp_gmres_restart": "50", "-pc_type": "jacobi",
+                                           "-ksp_rtol": "1e-10"})
+    assert fem.solveFullyImplicit(max_steps=3) == 0
+    files = sorted(p.name for p in tmp_path.glob("LDC2Dquad10-*.vtu"))
+    assert files == ["LDC2Dquad10-000000.vtu", "LDC2Dquad10-000001.vtu", "LDC2Dquad10-000002.vtu"]
+    d = read_vtu_point_data(str(tmp_path / files[-1]))
+    s = fem.solution().reshape(-1, 3)
+    assert d["velocity"].shape == (121, 3)
+    assert np.allclose(d["velocity"][:, :2], s[:, :2], atol=1e-6) and np.all(d["velocity"][:, 2] == 0)
+    assert np.allclose(d["pressure"], s[:, 2], atol=1e-6)
+    lines = [l for l in open(str(tmp_path / "LDC2Dquad10-forces.dat")).read().split("\n") if l.strip()]
+    assert len(lines) == 3 and lines[0].startswith("0.10000000000000")
