@@ -21,6 +21,9 @@ EXPORTS = [
     "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
     "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
     "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual", "cfdgpu_residual_norm_noalloc",
+    "cfdgpu_mpnn_create", "cfdgpu_mpnn_destroy", "cfdgpu_mpnn_num_params", "cfdgpu_mpnn_get_params",
+    "cfdgpu_mpnn_set_params", "cfdgpu_mpnn_set_scales", "cfdgpu_mpnn_add_sample", "cfdgpu_mpnn_num_samples",
+    "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess",
 ]
 KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
 
@@ -53,7 +56,8 @@ class StepStats(ctypes.Structure):
     _fields_ = [("newton_iters", ctypes.c_int), ("converged", ctypes.c_int),
                 ("norms", ctypes.c_double * MAX_NEWTON), ("ksp_its", ctypes.c_int * MAX_NEWTON),
                 ("ksp_reason", ctypes.c_int * MAX_NEWTON), ("refinements", ctypes.c_int * MAX_NEWTON),
-                ("ms_assembly", ctypes.c_double), ("ms_solver", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_assembly", ctypes.c_double), ("ms_solver", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("guess_used", ctypes.c_int), ("guess_norm", ctypes.c_double), ("plain_norm", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         n = self.newton_iters
@@ -61,7 +65,8 @@ class StepStats(ctypes.Structure):
         return {"newton_iters": n, "converged": bool(self.converged), "norms": list(self.norms[:n]),
                 "ksp_its": list(self.ksp_its[:nsolve]), "ksp_reason": list(self.ksp_reason[:nsolve]),
                 "refinements": list(self.refinements[:nsolve]), "ms_assembly": self.ms_assembly,
-                "ms_solver": self.ms_solver, "ms_total": self.ms_total}
+                "ms_solver": self.ms_solver, "ms_total": self.ms_total, "guess_used": bool(self.guess_used),
+                "guess_norm": self.guess_norm, "plain_norm": self.plain_norm}
 
 
 class PatternInfo(ctypes.Structure):
@@ -106,6 +111,18 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_timers.argtypes = [vp, vp]
     L.cfdgpu_true_residual.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
     L.cfdgpu_residual_norm_noalloc.argtypes = [ip, ip, vp, vp, vp, vp, vp, vp, vp]
+    L.cfdgpu_mpnn_create.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.cfdgpu_mpnn_destroy.argtypes = [vp]
+    L.cfdgpu_mpnn_num_params.argtypes = [vp]
+    L.cfdgpu_mpnn_get_params.argtypes = [vp, vp]
+    L.cfdgpu_mpnn_set_params.argtypes = [vp, vp]
+    L.cfdgpu_mpnn_set_scales.argtypes = [vp, vp, vp]
+    L.cfdgpu_mpnn_add_sample.argtypes = [vp, vp, vp, vp]
+    L.cfdgpu_mpnn_num_samples.argtypes = [vp]
+    L.cfdgpu_mpnn_loss_grad.argtypes = [vp, ip, vp, vp]
+    L.cfdgpu_mpnn_train.argtypes = [vp, ip, ctypes.c_float, vp]
+    L.cfdgpu_mpnn_predict.argtypes = [vp, vp, vp, vp]
+    L.cfdgpu_set_guess.argtypes = [vp, vp]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
     L.cfdgpu_set_profiling.argtypes = [vp, ip]
@@ -322,3 +339,85 @@ class Handle:
         self._check(self._L.cfdgpu_kernel_stats(self.h, KIND[kind], ctypes.byref(n), ctypes.byref(ms),
                                                 ctypes.byref(by)))
         return int(n.value), float(ms.value), float(by.value)
+
+
+class Mpnn:
+    """Learned Newton initial guess on a handle's mesh graph (cfdgpu_mpnn_*)."""
+
+    def __init__(self, handle: Handle, seed: int = 0):
+        self._L = handle._L
+        self.handle = handle
+        self.m = ctypes.c_void_p()
+        rc = self._L.cfdgpu_mpnn_create(handle.h, seed, ctypes.byref(self.m))
+        if rc != 0:
+            self._L.cfdgpu_mpnn_destroy(self.m)
+            self.m = ctypes.c_void_p()
+            raise CfdGpuError(rc, "cfdgpu_mpnn_create failed")
+        self.n = handle.n
+        self.ndof = handle.ndof
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CfdGpuError(rc, "mpnn call failed")
+
+    def close(self):
+        if self.m:
+            self._L.cfdgpu_mpnn_destroy(self.m)
+            self.m = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_params(self) -> int:
+        return int(self._L.cfdgpu_mpnn_num_params(self.m))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params, np.float32)
+        self._check(self._L.cfdgpu_mpnn_get_params(self.m, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        q = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self._L.cfdgpu_mpnn_set_params(self.m, _ptr(q)))
+
+    def set_scales(self, in_scale, out_scale):
+        a = np.ascontiguousarray(in_scale, dtype=np.float32)
+        b = np.ascontiguousarray(out_scale, dtype=np.float32)
+        self._check(self._L.cfdgpu_mpnn_set_scales(self.m, _ptr(a), _ptr(b)))
+
+    def add_sample(self, u_nm1, u_n, u_np1):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u_nm1, u_n, u_np1)]
+        self._check(self._L.cfdgpu_mpnn_add_sample(self.m, *[_ptr(a) for a in arrs]))
+
+    @property
+    def num_samples(self) -> int:
+        return int(self._L.cfdgpu_mpnn_num_samples(self.m))
+
+    def loss_grad(self, sample: int):
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self.num_params, np.float32)
+        self._check(self._L.cfdgpu_mpnn_loss_grad(self.m, sample, _ptr(loss), _ptr(g)))
+        return float(loss[0]), g
+
+    def train(self, iters: int, lr: float = 1e-3) -> float:
+        loss = np.zeros(1, np.float32)
+        self._check(self._L.cfdgpu_mpnn_train(self.m, iters, ctypes.c_float(lr), _ptr(loss)))
+        return float(loss[0])
+
+    def predict(self, u_nm1, u_n) -> np.ndarray:
+        a = np.ascontiguousarray(u_nm1, dtype=np.float64)
+        b = np.ascontiguousarray(u_n, dtype=np.float64)
+        d = np.zeros(self.n)
+        self._check(self._L.cfdgpu_mpnn_predict(self.m, _ptr(a), _ptr(b), _ptr(d)))
+        return d
+
+    def attach(self):
+        """Use this network as the handle's Newton initial guess."""
+        self._check(self._L.cfdgpu_set_guess(self.handle.h, self.m))
+
+    def detach(self):
+        self._check(self._L.cfdgpu_set_guess(self.handle.h, None))

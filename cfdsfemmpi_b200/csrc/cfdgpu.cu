@@ -21,6 +21,7 @@
 
 #include "../../include/cfdgpu.h"
 #include "element_kernels.cuh"
+#include "internal.h"
 #include "linalg_kernels.cuh"
 #include "setup.h"
 
@@ -82,6 +83,9 @@ struct cfdgpu_handle {
   GmresState *h_gst = nullptr;       // pinned
   bool assembled_K = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // learned initial guess
+  cfdgpu_mpnn *guess = nullptr;
+  double *guess_delta = nullptr, *rhs_plain = nullptr;
   // per-kernel event timing
   bool prof = false;
   std::vector<cudaEvent_t> pev;          // pool of 2*PROF_POOL events
@@ -546,7 +550,8 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
       if (reason_out) *reason_out = reason;
       return 0;
     }
-    if ((rc = restart())) return rc;
+    rc = restart();
+    if (rc != 0) return rc;
   }
 }
 
@@ -654,6 +659,17 @@ static int check_negjac(cfdgpu_handle *h)
   }
   return 0;
 }
+
+namespace cfdgpu {
+int handle_graph(cfdgpu_handle *h, GraphView *out)
+{
+  if (!h || !out) return CFDGPU_EINVAL;
+  out->nNode = h->nNode; out->ndof = h->ndof; out->ndim = h->ndim; out->nfree = h->topo.nfree;
+  out->rowptr = h->rowptr; out->colidx = h->colidx; out->coords = h->coords; out->fixmask = h->fixmask;
+  out->stream = h->stream;
+  return 0;
+}
+}  // namespace cfdgpu
 
 extern "C" {
 
@@ -823,6 +839,32 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     if ((rc = update_iter_step(h))) return rc;
     const bool want_K = !reuse || iter == 0;
     if ((rc = assemble(h, iter, want_K))) return rc;
+    if (iter == 0 && h->guess) {
+      // iteration-0 residual at the network's guess u_n + delta (free dofs);
+      // kept only if its norm does not exceed the constant predictor's
+      double nplain = 0.0, nguess = 0.0;
+      if ((rc = norm2(h, h->rhs, &nplain))) return rc;
+      CK(cudaMemcpyAsync(h->rhs_plain, h->rhs, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+      if ((rc = cfdgpu::mpnn_predict_increment(h->guess, h->prev, h->prev2, h->guess_delta, h->stream))) {
+        h->err = "guess network failed";
+        return rc;
+      }
+      k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0, h->guess_delta, h->soln);
+      LAUNCHED(h);
+      if ((rc = update_iter_step(h))) return rc;
+      if ((rc = assemble(h, 0, false))) return rc;
+      if ((rc = norm2(h, h->rhs, &nguess))) return rc;
+      stats->plain_norm = nplain;
+      stats->guess_norm = nguess;
+      if (nguess <= nplain) {
+        stats->guess_used = 1;
+      } else {
+        // back to the constant predictor: soln = u_n exactly, its residual
+        CK(cudaMemcpyAsync(h->soln, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->rhs, h->rhs_plain, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = update_iter_step(h))) return rc;
+      }
+    }
     if (iter == 0 && nfix) {
       k_dirichlet_update<<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->fixed_dofs, h->dbc_mult, h->applied, h->soln);
       LAUNCHED(h);
@@ -868,6 +910,18 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
   h->timers[1] += ms_asm * 1e-3;
   h->timers[2] += ms_sol * 1e-3;
   h->timers[4] += stats->ms_total * 1e-3;
+  return 0;
+}
+
+int cfdgpu_set_guess(cfdgpu_handle *h, cfdgpu_mpnn *m)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (m && !h->guess_delta) {
+    int rc;
+    if ((rc = dalloc(h, &h->guess_delta, (size_t)h->n))) return rc;
+    if ((rc = dalloc(h, &h->rhs_plain, (size_t)h->n))) return rc;
+  }
+  h->guess = m;
   return 0;
 }
 

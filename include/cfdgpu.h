@@ -108,6 +108,8 @@ typedef struct cfdgpu_step_stats {
   int ksp_reason[CFDGPU_MAX_NEWTON];    /* PETSc-style KSPConvergedReason per solve */
   int refinements[CFDGPU_MAX_NEWTON];   /* mixed mode: outer refinement passes per solve */
   double ms_assembly, ms_solver, ms_total;
+  int guess_used;                       /* 1: the network's initial guess was kept */
+  double guess_norm, plain_norm;        /* iteration-0 residual norms of both guesses (when a model is set) */
 } cfdgpu_step_stats;
 
 typedef struct cfdgpu_handle cfdgpu_handle;
@@ -221,6 +223,37 @@ int cfdgpu_timers(cfdgpu_handle *h, double t[5]);
 
 /* Number of kernel launches issued by this handle so far. */
 int64_t cfdgpu_launch_count(cfdgpu_handle *h);
+
+/* ---- learned Newton initial guess ------------------------------------
+ * A message-passing network over the handle's node graph (hidden width 64,
+ * three residual mean-aggregation layers) maps [u_n, u_n - u_{n-1}, X] to the
+ * next-step increment.  Training and inference run on the device with the
+ * library's own kernels (BF16 tensor-core GEMMs, FP32 accumulation, FP32
+ * Adam).  No counterpart in the reference: its Newton loop starts from the
+ * previous step's solution (src/base/StabFEM2.cpp:654, SolutionData.cpp:64-78). */
+typedef struct cfdgpu_mpnn cfdgpu_mpnn;
+int cfdgpu_mpnn_create(cfdgpu_handle *h, uint64_t seed, cfdgpu_mpnn **out);
+int cfdgpu_mpnn_destroy(cfdgpu_mpnn *m);
+int cfdgpu_mpnn_num_params(cfdgpu_mpnn *m);
+int cfdgpu_mpnn_get_params(cfdgpu_mpnn *m, float *p);
+int cfdgpu_mpnn_set_params(cfdgpu_mpnn *m, const float *p);
+/* feature scales for u_n and u_n - u_{n-1} (2*ndof values) and target
+ * scales (ndof values); set before adding samples */
+int cfdgpu_mpnn_set_scales(cfdgpu_mpnn *m, const float *in_scale, const float *out_scale);
+/* one training sample (host arrays of nNode*ndof): u_{n-1}, u_n, u_{n+1} */
+int cfdgpu_mpnn_add_sample(cfdgpu_mpnn *m, const double *u_nm1, const double *u_n, const double *u_np1);
+int cfdgpu_mpnn_num_samples(cfdgpu_mpnn *m);
+/* masked mean-squared error of one sample and its gradient (host floats) */
+int cfdgpu_mpnn_loss_grad(cfdgpu_mpnn *m, int sample, float *loss, float *grad);
+/* iters Adam steps cycling over the samples; *loss_out = last loss */
+int cfdgpu_mpnn_train(cfdgpu_mpnn *m, int iters, float lr, float *loss_out);
+/* predicted increment (host arrays; zero at prescribed dofs) */
+int cfdgpu_mpnn_predict(cfdgpu_mpnn *m, const double *u_nm1, const double *u_n, double *delta);
+/* use the network as the Newton initial guess of cfdgpu_step (NULL: the
+ * reference's constant predictor).  Each step evaluates the iteration-0
+ * residual at both guesses and keeps the network's only if its norm is not
+ * larger (stats->guess_used). */
+int cfdgpu_set_guess(cfdgpu_handle *h, cfdgpu_mpnn *m);
 
 /* Per-kernel device timing with CUDA events on the handle's stream (off by
  * default).  Kinds: */
