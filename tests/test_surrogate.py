@@ -117,25 +117,31 @@ def test_trained_guess_reduces_work_and_keeps_the_answer():
     inner GMRES iterations drop, and every step still meets the 1e-8
     residual; the fields agree with the run without the guess."""
     mesh, ctrl, _ = meshgen.case_hex(8, 16)
-    traj, _ = collect_trajectory(mesh, ctrl, 10, restart=400, rtol=1e-10, pc="pbjacobi")
+    # plain trajectory to step 10, keeping the generalised-alpha history
+    h0 = Handle(mesh, ctrl, restart=400, rtol=1e-10, pc="pbjacobi")
+    traj = [np.zeros(h0.n)]
+    t = ctrl.dt
+    for _ in range(10):
+        h0.step(t, t if t <= 1.0 else 1.0)
+        traj.append(h0.get_solution())
+        t = t + ctrl.dt
+    prev10, dot10 = h0.get_history()
+    h0.close()
     kw = dict(restart=400, pc="pbjacobi", precision="mixed", inner_restart=100, inner_rtol=1e-4, max_it=40000)
     res = {}
     for use in (False, True):
         h = Handle(mesh, ctrl, **kw)
-        # start both runs from the trajectory state at step 10
         h.set_solution(traj[10])
-        dot = (traj[10] - traj[9]) / ctrl.dt * 1.0
-        h.set_history(traj[9], None)
+        h.set_history(prev10, dot10)
         net = None
         if use:
             net, losses = train_guess(h, traj, iters=1500, lr=2e-3, seed=2)
             net.attach()
-        t = 10 * ctrl.dt + ctrl.dt
+        tt = t
         st = []
-        # warm the generalised-alpha history by running one step first
         for _ in range(6):
-            st.append(h.step(t, t if t <= 1.0 else 1.0).as_dict())
-            t = t + ctrl.dt
+            st.append(h.step(tt, tt if tt <= 1.0 else 1.0).as_dict())
+            tt = tt + ctrl.dt
         res[use] = (h.get_solution(), st)
         if net is not None:
             net.close()
