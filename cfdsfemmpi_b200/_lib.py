@@ -57,7 +57,8 @@ class StepStats(ctypes.Structure):
                 ("norms", ctypes.c_double * MAX_NEWTON), ("ksp_its", ctypes.c_int * MAX_NEWTON),
                 ("ksp_reason", ctypes.c_int * MAX_NEWTON), ("refinements", ctypes.c_int * MAX_NEWTON),
                 ("ms_assembly", ctypes.c_double), ("ms_solver", ctypes.c_double), ("ms_total", ctypes.c_double),
-                ("guess_used", ctypes.c_int), ("guess_norm", ctypes.c_double), ("plain_norm", ctypes.c_double)]
+                ("guess_used", ctypes.c_int), ("guess_norm", ctypes.c_double), ("plain_norm", ctypes.c_double),
+                ("guess_alpha", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         n = self.newton_iters
@@ -66,7 +67,7 @@ class StepStats(ctypes.Structure):
                 "ksp_its": list(self.ksp_its[:nsolve]), "ksp_reason": list(self.ksp_reason[:nsolve]),
                 "refinements": list(self.refinements[:nsolve]), "ms_assembly": self.ms_assembly,
                 "ms_solver": self.ms_solver, "ms_total": self.ms_total, "guess_used": bool(self.guess_used),
-                "guess_norm": self.guess_norm, "plain_norm": self.plain_norm}
+                "guess_norm": self.guess_norm, "plain_norm": self.plain_norm, "guess_alpha": self.guess_alpha}
 
 
 class PatternInfo(ctypes.Structure):

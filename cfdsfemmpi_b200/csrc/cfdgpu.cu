@@ -75,7 +75,7 @@ struct cfdgpu_handle {
   double *V = nullptr;
   GmresState *gst = nullptr;
   GmresArrays ga{};
-  double *red_partial = nullptr;
+  double *red_partial = nullptr, *red_partial2 = nullptr;
   unsigned int *red_counter = nullptr;
   double *scalar = nullptr;          // device scalar slots
   int *negjac = nullptr;
@@ -282,6 +282,13 @@ __global__ void k_round_f32(int64_t n4, const double *__restrict__ a, float *__r
     const double2 v = reinterpret_cast<const double2 *>(a)[2 * i + 1];
     reinterpret_cast<float4 *>(b)[i] = make_float4((float)u.x, (float)u.y, (float)v.x, (float)v.y);
   }
+}
+
+// y = a*x + b*y
+__global__ void k_lincomb(int64_t n, double a, const double *__restrict__ x, double b, double *__restrict__ y)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
 }
 
 __global__ void k_axpy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ y)
@@ -782,6 +789,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
   }
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
+  if ((rc = dalloc(h, &h->red_partial2, (size_t)2 * RED_BLOCKS))) return rc;
   if ((rc = dalloc(h, &h->red_counter, 1))) return rc;
   CK(cudaMemset(h->red_counter, 0, sizeof(unsigned int)));
   if ((rc = dalloc(h, &h->scalar, 8))) return rc;
@@ -840,9 +848,12 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     const bool want_K = !reuse || iter == 0;
     if ((rc = assemble(h, iter, want_K))) return rc;
     if (iter == 0 && h->guess) {
-      // iteration-0 residual at the network's guess u_n + delta (free dofs);
-      // kept only if its norm does not exceed the constant predictor's
-      double nplain = 0.0, nguess = 0.0;
+      // Network guess u_n + alpha*delta on the free dofs.  The iteration-0
+      // residual is affine in soln, F(u_n + alpha*delta) = F_A + alpha (F_B - F_A)
+      // with F_A at the constant predictor and F_B at alpha = 1, so alpha is
+      // chosen to minimise its norm; alpha <= 0 or no decrease keeps the
+      // constant predictor (the reference's guess) unchanged.
+      double nplain = 0.0;
       if ((rc = norm2(h, h->rhs, &nplain))) return rc;
       CK(cudaMemcpyAsync(h->rhs_plain, h->rhs, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
       if ((rc = cfdgpu::mpnn_predict_increment(h->guess, h->prev, h->prev2, h->guess_delta, h->stream))) {
@@ -853,17 +864,29 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
       LAUNCHED(h);
       if ((rc = update_iter_step(h))) return rc;
       if ((rc = assemble(h, 0, false))) return rc;
-      if ((rc = norm2(h, h->rhs, &nguess))) return rc;
+      minres_dots<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(h->n, h->rhs_plain, h->rhs, h->red_partial2, h->red_counter,
+                                                            h->scalar + 2);
+      LAUNCHED(h);
+      CK(cudaMemcpyAsync(h->h_scalar + 2, h->scalar + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      const double num = h->h_scalar[2], den = h->h_scalar[3];
+      const double alpha = (den > 0.0 && num > 0.0) ? num / den : 0.0;
+      const double nres2 = nplain * nplain - (den > 0.0 ? num * num / den : 0.0);
+      const double nguess = std::sqrt(std::max(nres2, 0.0));
       stats->plain_norm = nplain;
-      stats->guess_norm = nguess;
-      if (nguess <= nplain) {
+      stats->guess_norm = (alpha > 0.0) ? nguess : nplain;
+      // soln = u_n + alpha * delta, rhs = (1 - alpha) F_A + alpha F_B
+      CK(cudaMemcpyAsync(h->soln, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+      if (alpha > 0.0 && nguess < nplain) {
         stats->guess_used = 1;
+        stats->guess_alpha = alpha;
+        k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, alpha, h->guess_delta, h->soln);
+        k_lincomb<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0 - alpha, h->rhs_plain, alpha, h->rhs);
+        h->launches += 2;
       } else {
-        // back to the constant predictor: soln = u_n exactly, its residual
-        CK(cudaMemcpyAsync(h->soln, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
         CK(cudaMemcpyAsync(h->rhs, h->rhs_plain, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
-        if ((rc = update_iter_step(h))) return rc;
       }
+      if ((rc = update_iter_step(h))) return rc;
     }
     if (iter == 0 && nfix) {
       k_dirichlet_update<<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->fixed_dofs, h->dbc_mult, h->applied, h->soln);

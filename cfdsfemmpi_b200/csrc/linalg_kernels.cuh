@@ -357,6 +357,32 @@ template <> struct Chunk<float> {
   }
 };
 
+// out[0] = <a, a - b>, out[1] = ||a - b||^2 (deterministic; partial holds
+// 2 * gridDim.x doubles)
+__global__ void __launch_bounds__(RED_THREADS)
+minres_dots(int64_t n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ partial,
+            unsigned int *counter, double *__restrict__ out)
+{
+  __shared__ double sh[RED_THREADS / 32];
+  double s0 = 0.0, s1 = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
+    const double d = a[i] - b[i];
+    s0 = fma(a[i], d, s0);
+    s1 = fma(d, d, s1);
+  }
+  s0 = block_sum<RED_THREADS>(s0, sh);
+  s1 = block_sum<RED_THREADS>(s1, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s0; partial[2 * blockIdx.x + 1] = s1; }
+  if (last_block(counter, gridDim.x)) {
+    if (threadIdx.x == 0) {
+      double t0 = 0.0, t1 = 0.0;
+      for (unsigned int k = 0; k < gridDim.x; k++) { t0 += partial[2 * k]; t1 += partial[2 * k + 1]; }
+      out[0] = t0;
+      out[1] = t1;
+    }
+  }
+}
+
 // GMRES cycle start: res = ||V0||, convergence test at its, v0scale.
 template <typename VT>
 __global__ void __launch_bounds__(RED_THREADS)

@@ -110,6 +110,7 @@ typedef struct cfdgpu_step_stats {
   double ms_assembly, ms_solver, ms_total;
   int guess_used;                       /* 1: the network's initial guess was kept */
   double guess_norm, plain_norm;        /* iteration-0 residual norms of both guesses (when a model is set) */
+  double guess_alpha;                   /* step length along the predicted increment (0: constant predictor) */
 } cfdgpu_step_stats;
 
 typedef struct cfdgpu_handle cfdgpu_handle;
@@ -251,8 +252,10 @@ int cfdgpu_mpnn_train(cfdgpu_mpnn *m, int iters, float lr, float *loss_out);
 int cfdgpu_mpnn_predict(cfdgpu_mpnn *m, const double *u_nm1, const double *u_n, double *delta);
 /* use the network as the Newton initial guess of cfdgpu_step (NULL: the
  * reference's constant predictor).  Each step evaluates the iteration-0
- * residual at both guesses and keeps the network's only if its norm is not
- * larger (stats->guess_used). */
+ * residual at u_n and at u_n + delta; the residual is affine in the state, so
+ * the step length alpha minimising ||F(u_n + alpha*delta)|| is exact.  The
+ * network's guess is kept only if alpha > 0 lowers the residual
+ * (stats->guess_used); otherwise the step runs from the constant predictor. */
 int cfdgpu_set_guess(cfdgpu_handle *h, cfdgpu_mpnn *m);
 
 /* Per-kernel device timing with CUDA events on the handle's stream (off by
