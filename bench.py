@@ -368,9 +368,9 @@ def run_surrogate(args, world, rank, local):
     h0.close()
     t_traj = time.perf_counter() - T0
     results = {}
-    for name in ("plain", "surrogate", "reference_tight"):
+    for name in ("plain", "mixed_no_guess", "surrogate", "reference_tight"):
         kw = dict(opts)
-        if name == "surrogate":
+        if name in ("surrogate", "mixed_no_guess"):
             kw.update(precision="mixed", inner_restart=100, inner_rtol=1e-4, max_it=40000)
         if name == "reference_tight":
             kw.update(rtol=1e-12, max_it=40000)
@@ -429,13 +429,17 @@ def run_surrogate(args, world, rank, local):
             "plain_same_steps": {"value": args.steps / (pl["ms"] * 1e-3), "unit": "steps/s",
                                  "gmres_iters_per_step": statistics.mean(sum(s["ksp_its"]) for s in pl["stats"])},
             "speedup_vs_plain": pl["ms"] / sur["ms"],
+            "mixed_without_guess_same_steps": {
+                "value": args.steps / (results["mixed_no_guess"]["ms"] * 1e-3), "unit": "steps/s",
+                "gmres_iters_per_step": statistics.mean(sum(s["ksp_its"]) for s in results["mixed_no_guess"]["stats"])},
             "gmres_iters_per_step": statistics.mean(sum(s["ksp_its"]) for s in sur["stats"]),
             "newton_iters_per_step": statistics.mean(s["newton_iters"] for s in sur["stats"]),
             "guess_used_steps": sum(s["guess_used"] for s in sur["stats"]),
             "guess_residual_ratio": statistics.mean(s["guess_norm"] / s["plain_norm"] for s in sur["stats"]
                                                     if s["plain_norm"] > 0),
             "all_converged": all(s["converged"] for s in sur["stats"]),
-            "field_error_vs_fp64_rtol1e-12": {"surrogate_mixed": err(sur["soln"]), "plain_fp64": err(pl["soln"])},
+            "field_error_vs_fp64_rtol1e-12": {"surrogate_mixed": err(sur["soln"]), "plain_fp64": err(pl["soln"]),
+                                              "mixed_without_guess": err(results["mixed_no_guess"]["soln"])},
             "train_seconds": sur["t_train"], "trajectory_seconds": t_traj}
     return line
 
