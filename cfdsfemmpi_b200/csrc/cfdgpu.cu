@@ -72,6 +72,9 @@ struct cfdgpu_handle {
   double inner_rtol = 1e-4, refine_rtol = 1e-6;
   GmresState *gst32 = nullptr;
   GmresArrays ga32{};
+  // Arnoldi chunks captured as CUDA graphs (per Krylov space, per chunk start)
+  bool use_graphs = true;
+  std::vector<cudaGraphExec_t> graphs64, graphs32;
   double *V = nullptr;
   GmresState *gst = nullptr;
   GmresArrays ga{};
@@ -411,7 +414,8 @@ static double spmv_bytes(cfdgpu_handle *h, int mode, int vbytes, int mbytes, int
 }
 
 // y = M^-1 (A x) (mode 0) or y = M^-1 (b - A x) (mode 1), FP64 vectors
-static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y, const GmresState *st, int j)
+static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y, const GmresState *st, int j,
+                   const double *xscale = nullptr)
 {
   const int pc = h->opts.pc_type;
   const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, mode, 8, 8, pc));
@@ -419,7 +423,7 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
     const int grid = (int)((h->nNode * 32LL + 255) / 256);
 #define SPMV4(MO, PCV)                                                                                          \
   bsr4_spmv<MO, PCV, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, h->dinv, \
-                                                           h->binv, y, st, j)
+                                                           h->binv, y, st, j, xscale)
     if (mode == 0) {
       if (pc == 0) SPMV4(0, 0); else if (pc == 1) SPMV4(0, 1); else SPMV4(0, 2);
     } else {
@@ -430,7 +434,7 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
     const int grid = (int)((h->n + 255) / 256);
 #define SPMV3(MO, PCV)                                                                                        \
   bsr_spmv_generic<3, MO, PCV, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, \
-                                                                     h->dinv, h->binv, y, st, j)
+                                                                     h->dinv, h->binv, y, st, j, xscale)
     if (mode == 0) {
       if (pc == 0) SPMV3(0, 0); else if (pc == 1) SPMV3(0, 1); else SPMV3(0, 2);
     } else {
@@ -444,17 +448,17 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
 }
 
 // y = M32^-1 (A32 x), FP32 vectors (mixed-precision inner solve)
-static int spmv32_pc(cfdgpu_handle *h, const float *x, float *y, const GmresState *st, int j)
+static int spmv32_pc(cfdgpu_handle *h, const float *x, float *y, const GmresState *st, int j, const double *xscale)
 {
   const int pc = h->opts.pc_type;
   const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 0, 4, 4, pc));
   const int grid = (int)((h->nNode * 32LL + 255) / 256);
   if (pc == 0)
-    bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j);
+    bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
   else if (pc == 1)
-    bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j);
+    bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
   else
-    bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j);
+    bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
   prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "bsr_spmv_f32");
@@ -485,6 +489,8 @@ struct Krylov {
   int64_t ldv = 0;
   GmresState *st = nullptr;
   GmresArrays ga{};
+  std::vector<cudaGraphExec_t> &graphs;
+  explicit Krylov(std::vector<cudaGraphExec_t> &g) : graphs(g) {}
 };
 
 // Restarted GMRES with PETSc semantics on a Krylov space.  The caller has
@@ -501,7 +507,7 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
   const int64_t ldv = K.ldv;
   const int64_t nchunk = ldv / E;
   const int ntiles = (int)((nchunk + ORTHO_THREADS - 1) / ORTHO_THREADS);
-  const int mtiles = (int)((nchunk + MAXPY_CHUNKS - 1) / MAXPY_CHUNKS);
+  const int mtiles = (int)(nchunk / MAXPY_SPAN);
   VT *V = K.V;
   GmresState *st = K.st;
   int rc;
@@ -509,29 +515,53 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
   LAUNCHED(h);
   CK(cudaMemsetAsync(x, 0, sizeof(double) * n, h->stream));
   const int vgrid = grid_for(n);
-  const int pgrid = grid_for(nchunk);
+  // Arnoldi steps j0..j0+CH-1 enqueued as one unit: directly, or (without
+  // per-kernel profiling) as a CUDA graph captured once per chunk and reused
+  const int CH = 8;
+  auto enqueue_chunk = [&](int j0) -> int {
+    for (int j = j0; j < std::min(m, j0 + CH); j++) {
+      int r;
+      if ((r = arnoldi(j))) return r;
+      const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 3.0) * (double)sizeof(VT) * n);
+      dim3 g2(ntiles, (j + 1 + MDOT_KC - 1) / MDOT_KC);
+      gmres_mdot<VT><<<g2, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga.partial);
+      gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, K.ga.partial, K.ga.H, K.ga.sigma);
+      gmres_maxpy_norm<VT><<<mtiles, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga);
+      prof_end(h, pi);
+    }
+    return check_launch(h, "gmres_arnoldi");
+  };
   while (true) {
     gmres_start<VT><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, st, K.ga);
-    scale_v0<VT><<<vgrid, 256, 0, h->stream>>>(n, V, st);
-    h->launches += 2;
+    h->launches += 1;
     if ((rc = check_launch(h, "gmres_start"))) return rc;
-    // Arnoldi steps; poll the device flag one chunk behind so the GPU stays fed
-    const int CH = 8;
+    // poll the device flag one chunk behind so the GPU stays fed
     bool stop = false;
     cudaEvent_t evs[2] = {h->ev0, h->ev1};
     for (int j0 = 0; j0 < m && !stop; j0 += CH) {
-      for (int j = j0; j < std::min(m, j0 + CH); j++) {
-        if ((rc = arnoldi(j))) return rc;
-        const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 5.0) * (double)sizeof(VT) * n);
-        dim3 g2(ntiles, (j + 1 + MDOT_KC - 1) / MDOT_KC);
-        gmres_mdot<VT><<<g2, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga.partial);
-        gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, K.ga.partial, K.ga.H);
-        gmres_maxpy_norm<VT><<<mtiles, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga);
-        prof_end(h, pi);
-        gmres_scale_next<VT><<<pgrid, 256, 0, h->stream>>>(nchunk, V, ldv, j, st);
-        h->launches += 4;
+      const int nk = std::min(m, j0 + CH) - j0;
+      if (h->use_graphs && !h->prof) {
+        std::vector<cudaGraphExec_t> &cache = K.graphs;
+        if (cache.size() < (size_t)((m + CH - 1) / CH)) cache.resize((m + CH - 1) / CH, nullptr);
+        cudaGraphExec_t &ex = cache[j0 / CH];
+        if (!ex) {
+          cudaGraph_t g = nullptr;
+          CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+          const int64_t before = h->launches;
+          const int r = enqueue_chunk(j0);
+          const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+          if (r) return r;
+          if (ec != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(ec); return CFDGPU_ECUDA; }
+          CK(cudaGraphInstantiate(&ex, g, 0));
+          CK(cudaGraphDestroy(g));
+          h->launches = before;   // counted when the graph runs
+        }
+        CK(cudaGraphLaunch(ex, h->stream));
+        h->launches += 4 * nk;
+      } else {
+        if ((rc = enqueue_chunk(j0))) return rc;
+        h->launches += 4 * nk;
       }
-      if ((rc = check_launch(h, "gmres_arnoldi"))) return rc;
       const int cidx = (j0 / CH) & 1;
       CK(cudaMemcpyAsync(&h->h_gst[cidx], st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
       CK(cudaEventRecord(evs[cidx], h->stream));
@@ -571,10 +601,12 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
   else
     pc_apply<3, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, h->V);
   LAUNCHED(h);
-  Krylov<double> K;
+  Krylov<double> K(h->graphs64);
   K.V = h->V; K.m = h->m; K.ldv = h->ldv; K.st = h->gst; K.ga = h->ga;
-  auto arn = [&](int j) { return spmv_pc(h, 0, h->V + (int64_t)j * h->ldv, nullptr, h->V + (int64_t)(j + 1) * h->ldv, h->gst, j); };
-  auto res = [&]() { return spmv_pc(h, 1, x, b, h->V, nullptr, 0); };
+  auto arn = [&](int j) {
+    return spmv_pc(h, 0, h->V + (int64_t)j * h->ldv, nullptr, h->V + (int64_t)(j + 1) * h->ldv, h->gst, j, h->ga.sigma + j);
+  };
+  auto res = [&]() { return spmv_pc(h, 1, x, b, h->V, nullptr, 0, nullptr); };
   return gmres_run<double>(h, K, x, h->opts.max_it, h->opts.rtol, h->opts.atol, h->opts.dtol, false, arn, res,
                            its_out, reason_out);
 }
@@ -600,7 +632,7 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
   const double target = std::max(h->refine_rtol * bnorm, 0.1 * h->ctrl.newton_tol);
   int total = 0, passes = 0, reason = 2;
   double rn = bnorm;
-  Krylov<float> K;
+  Krylov<float> K(h->graphs32);
   K.V = h->V32; K.m = h->m32; K.ldv = h->ldv; K.st = h->gst32; K.ga = h->ga32;
   const int max_passes = 100;
   while (rn > target && passes < max_passes && total < h->opts.max_it) {
@@ -610,7 +642,9 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
     pc_apply<4, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
     h->launches += 2;
     if ((rc = check_launch(h, "mixed_prepare"))) return rc;
-    auto arn = [&](int j) { return spmv32_pc(h, h->V32 + (int64_t)j * h->ldv, h->V32 + (int64_t)(j + 1) * h->ldv, h->gst32, j); };
+    auto arn = [&](int j) {
+      return spmv32_pc(h, h->V32 + (int64_t)j * h->ldv, h->V32 + (int64_t)(j + 1) * h->ldv, h->gst32, j, h->ga32.sigma + j);
+    };
     auto nores = [&]() { return 0; };
     int its = 0, r = 0;
     if ((rc = gmres_run<float>(h, K, h->d64, h->m32, h->inner_rtol, 1e-50, 1e4, true, arn, nores, &its, &r)))
@@ -624,7 +658,7 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
       const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 1, 8, 4, 0));
       const int grid = (int)((h->nNode * 32LL + 255) / 256);
       bsr4_spmv<1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b, nullptr,
-                                                           nullptr, h->r64, nullptr, 0);
+                                                           nullptr, h->r64, nullptr, 0, nullptr);
       prof_end(h, pi);
       LAUNCHED(h);
       if ((rc = check_launch(h, "mixed_residual"))) return rc;
@@ -743,7 +777,8 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   const size_t bb = (size_t)h->ndof * h->ndof;
   h->mixed = (h->opts.precision == CFDGPU_PREC_MIXED);
   if (h->mixed && h->ndof != 4) { h->err = "mixed precision is built for the 4x4-block (3D) systems"; return CFDGPU_EINVAL; }
-  h->ldv = (n + 31) / 32 * 32;
+  // Krylov stride: a multiple of 512 entries, so every update CTA covers whole chunks
+  h->ldv = (n + 511) / 512 * 512;
   if (h->mixed) {
     // FP32 tangent and FP32 inner Krylov space; the FP64 matrix is not stored
     h->m32 = (h->opts.inner_restart > 0) ? h->opts.inner_restart : 100;
@@ -764,11 +799,12 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = dalloc(h, &h->gst32, 1))) return rc;
     CK(cudaMemset(h->gst32, 0, sizeof(GmresState)));
     if ((rc = dalloc(h, &h->ga32.H, (size_t)(h->m32 + 1) * h->m32))) return rc;
+    if ((rc = dalloc(h, &h->ga32.sigma, (size_t)h->m32 + 1))) return rc;
     if ((rc = dalloc(h, &h->ga32.cs, (size_t)h->m32))) return rc;
     if ((rc = dalloc(h, &h->ga32.sn, (size_t)h->m32))) return rc;
     if ((rc = dalloc(h, &h->ga32.grs, (size_t)h->m32 + 1))) return rc;
     if ((rc = dalloc(h, &h->ga32.y, (size_t)h->m32))) return rc;
-    const int64_t nt32 = (h->ldv / 4 + MAXPY_CHUNKS - 1) / MAXPY_CHUNKS;
+    const int64_t nt32 = (h->ldv / 4 + ORTHO_THREADS - 1) / ORTHO_THREADS + h->ldv / 4 / MAXPY_SPAN + 1;
     if ((rc = dalloc(h, &h->ga32.partial, (size_t)(h->m32 + 1) * std::max<int64_t>(nt32, RED_BLOCKS)))) return rc;
   } else {
     if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
@@ -780,12 +816,13 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   CK(cudaMemset(h->V, 0, sizeof(double) * h->ldv * (h->m + 1)));
   if ((rc = dalloc(h, &h->gst, 1))) return rc;
   if ((rc = dalloc(h, &h->ga.H, (size_t)(h->m + 1) * h->m))) return rc;
+  if ((rc = dalloc(h, &h->ga.sigma, (size_t)h->m + 1))) return rc;
   if ((rc = dalloc(h, &h->ga.cs, (size_t)h->m))) return rc;
   if ((rc = dalloc(h, &h->ga.sn, (size_t)h->m))) return rc;
   if ((rc = dalloc(h, &h->ga.grs, (size_t)h->m + 1))) return rc;
   if ((rc = dalloc(h, &h->ga.y, (size_t)h->m))) return rc;
   {
-    const int64_t ntiles = (h->ldv / 2 + MAXPY_CHUNKS - 1) / MAXPY_CHUNKS;
+    const int64_t ntiles = (h->ldv / 2 + ORTHO_THREADS - 1) / ORTHO_THREADS + h->ldv / 2 / MAXPY_SPAN + 1;
     if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
   }
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
@@ -811,6 +848,8 @@ int cfdgpu_destroy(cfdgpu_handle *h)
   if (h->h_scalar) cudaFreeHost(h->h_scalar);
   if (h->h_gst) cudaFreeHost(h->h_gst);
   for (auto &e : h->pev) cudaEventDestroy(e);
+  for (auto g : h->graphs64) if (g) cudaGraphExecDestroy(g);
+  for (auto g : h->graphs32) if (g) cudaGraphExecDestroy(g);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1114,7 +1153,7 @@ int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, dou
   CK(cudaMemcpyAsync(h->rhs, b, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
   const int saved_pc = h->opts.pc_type;
   h->opts.pc_type = CFDGPU_PC_NONE;
-  int rc = spmv_pc(h, 1, h->dx, h->rhs, h->V, nullptr, 0);
+  int rc = spmv_pc(h, 1, h->dx, h->rhs, h->V, nullptr, 0, nullptr);
   h->opts.pc_type = saved_pc;
   if (rc) return rc;
   return norm2(h, h->V, norm);
@@ -1219,11 +1258,11 @@ extern "C" int cfdgpu_residual_norm_noalloc(int nNode, int ndof, const int32_t *
   if (ndof == 4) {
     const int grid = (int)((nNode * 32LL + 255) / 256);
     bsr4_spmv<1, 0, double><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr, nullptr, r,
-                                                nullptr, 0);
+                                                nullptr, 0, nullptr);
   } else {
     const int grid = (int)((n + 255) / 256);
     bsr_spmv_generic<3, 1, 0, double><<<grid, 256, 0, s>>>(nNode, d_rowptr, d_colidx, d_val, d_x, d_b, nullptr,
-                                                             nullptr, r, nullptr, 0);
+                                                             nullptr, r, nullptr, 0, nullptr);
   }
   if (cudaGetLastError() != cudaSuccess) return CFDGPU_ECUDA;
   norm2_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, r, partial, counter, d_norm);

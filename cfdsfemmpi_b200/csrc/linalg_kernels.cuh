@@ -32,11 +32,12 @@ struct GmresState {
   double rnorm0, ttol;
   double res;      // current residual-norm estimate
   double tt;       // norm of the newest Krylov vector
-  double v0scale;  // 1/res for V_0 (0: leave V_0 as is)
+  double v0scale;  // 1/res for V_0 (kept for diagnostics; sigma[0] holds the scale)
   unsigned int counter;
 };
 
 struct GmresArrays {
+  double *sigma;   // m+1: basis vector k is sigma[k] * V_k (the stored vectors are not normalised)
   double *H;       // (m+1) x m, column-major, see hidx()
   double *cs, *sn; // m
   double *grs;     // m+1
@@ -105,12 +106,13 @@ __global__ void __launch_bounds__(256)
 bsr4_spmv(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
               const MT *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
               const double *__restrict__ dinv, const double *__restrict__ binv, double *__restrict__ y,
-              const GmresState *__restrict__ st, int j)
+              const GmresState *__restrict__ st, int j, const double *__restrict__ xscale)
 {
   if (st && (!st->active || st->it != j)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nrows) return;
+  const double xs = xscale ? xscale[0] : 1.0;
   const int sub = lane >> 3, q = lane & 7, row = q >> 1, cp = (q & 1) * 2;
   const int kb0 = rowptr[warp], kb1 = rowptr[warp + 1];
   double acc0 = 0.0, acc1 = 0.0;
@@ -132,6 +134,7 @@ bsr4_spmv(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restri
   acc += __shfl_xor_sync(0xffffffffu, acc, 1);
   acc += __shfl_xor_sync(0xffffffffu, acc, 8);
   acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+  acc *= xs;
   // lanes 0,2,4,6 hold rows 0..3
   const int64_t r = (int64_t)warp * 4 + row;
   double v = acc;
@@ -156,12 +159,14 @@ template <int PC>
 __global__ void __launch_bounds__(256)
 bsr4_spmv_f32(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
               const float *__restrict__ val, const float *__restrict__ x, const float *__restrict__ dinv,
-              const float *__restrict__ binv, float *__restrict__ y, const GmresState *__restrict__ st, int j)
+              const float *__restrict__ binv, float *__restrict__ y, const GmresState *__restrict__ st, int j,
+              const double *__restrict__ xscale)
 {
   if (st && (!st->active || st->it != j)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nrows) return;
+  const float xs = xscale ? (float)xscale[0] : 1.f;
   const int sub = lane >> 2, row = lane & 3;
   const int kb0 = rowptr[warp], kb1 = rowptr[warp + 1];
   float acc = 0.f;
@@ -177,6 +182,7 @@ bsr4_spmv_f32(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__re
   acc += __shfl_xor_sync(0xffffffffu, acc, 4);
   acc += __shfl_xor_sync(0xffffffffu, acc, 8);
   acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+  acc *= xs;
   const int64_t r = (int64_t)warp * 4 + row;
   if (PC == 2) {
     const float v0 = __shfl_sync(0xffffffffu, acc, 0), v1 = __shfl_sync(0xffffffffu, acc, 1);
@@ -196,9 +202,11 @@ template <int NB, int MODE, int PC, typename VT>
 __global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
                                  const VT *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
                                  const double *__restrict__ dinv, const double *__restrict__ binv,
-                                 double *__restrict__ y, const GmresState *__restrict__ st, int j)
+                                 double *__restrict__ y, const GmresState *__restrict__ st, int j,
+                                 const double *__restrict__ xscale)
 {
   if (st && (!st->active || st->it != j)) return;
+  const double xs = xscale ? xscale[0] : 1.0;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t node = t / NB;
   const int row = (int)(t % NB);
@@ -210,7 +218,7 @@ __global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, 
 #pragma unroll
     for (int q = 0; q < NB; q++) acc = fma((double)a[q], x[(int64_t)c * NB + q], acc);
   }
-  double v = (MODE == 1) ? b[t] - acc : acc;
+  double v = (MODE == 1) ? b[t] - xs * acc : xs * acc;
   if (PC == 1) v *= dinv[t];
   if (PC == 2) {
     // point block needs the whole node: recompute the node's other rows
@@ -224,7 +232,7 @@ __global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, 
 #pragma unroll
         for (int q = 0; q < NB; q++) s = fma((double)a[q], x[(int64_t)c * NB + q], s);
       }
-      vv[rr] = (MODE == 1) ? b[node * NB + rr] - s : s;
+      vv[rr] = (MODE == 1) ? b[node * NB + rr] - xs * s : xs * s;
     }
     double z = 0.0;
 #pragma unroll
@@ -405,6 +413,7 @@ gmres_start(int64_t n, const VT *__restrict__ v0, GmresState *st, GmresArrays ga
       st->it = 0;
       ga.grs[0] = res;
       st->v0scale = (res != 0.0) ? 1.0 / res : 0.0;
+      ga.sigma[0] = (res != 0.0) ? 1.0 / res : 1.0;
       if (res == 0.0) {
         if (st->its == 0) { st->rnorm0 = 0.0; st->ttol = st->atol; }
         st->reason = 3;   // KSP_CONVERGED_ATOL: zero residual on entry
@@ -415,15 +424,6 @@ gmres_start(int64_t n, const VT *__restrict__ v0, GmresState *st, GmresArrays ga
       }
     }
   }
-}
-
-template <typename VT>
-__global__ void scale_v0(int64_t n, VT *__restrict__ v0, const GmresState *__restrict__ st)
-{
-  const double s = st->v0scale;
-  if (s == 0.0) return;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v0[i] = (VT)((double)v0[i] * s);
 }
 
 // Hessenberg storage: column-major, leading dimension m+1: H(r, c) = H[c*(m+1) + r].
@@ -484,9 +484,11 @@ gmres_mdot(int64_t nchunk, const VT *__restrict__ V, int64_t ldv, int j, const G
   }
 }
 
-// pass 2: one warp per k sums the tile partials in a fixed order -> H(k, j)
+// pass 2: one warp per k sums the tile partials in a fixed order and scales by
+// the stored vector's sigma -> H(k, j) = <w, sigma_k V_k>
 __global__ void gmres_mdot_reduce(int ntiles, int j, const GmresState *__restrict__ st,
-                                  const double *__restrict__ partial, double *__restrict__ H)
+                                  const double *__restrict__ partial, double *__restrict__ H,
+                                  const double *__restrict__ sigma)
 {
   if (!st->active || st->it != j) return;
   const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -497,16 +499,19 @@ __global__ void gmres_mdot_reduce(int ntiles, int j, const GmresState *__restric
   for (int b = lane; b < ntiles; b += 32) t += pp[b];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-  if (lane == 0) H[hidx(k, j, st->m)] = t;
+  if (lane == 0) H[hidx(k, j, st->m)] = sigma[k] * t;
 }
 
-// w -= sum_k H(k, j) V_k, then ||w||^2 partials.  A CTA covers MAXPY_CHUNKS
-// 16-byte chunks; its four thread quarters take the k's congruent to 0..3
-// mod 4 (consecutive lanes on consecutive chunks), and the quarter sums are
-// combined in a fixed order through shared memory.  The last CTA finishes the
-// norm, applies the stored Givens rotations to column j, forms the new one and
-// runs the convergence test (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
+// w -= sum_k h_k sigma_k V_k, then ||w||^2 partials.  A CTA covers
+// 2*MAXPY_CHUNKS 16-byte chunks: each thread owns two chunks (lp and
+// lp + MAXPY_CHUNKS, two independent load streams), its quarter of the CTA
+// takes the k's congruent to 0..3 mod 4 (consecutive lanes on consecutive
+// chunks), and the quarter sums are combined in a fixed order through shared
+// memory.  The last CTA finishes the norm, applies the stored Givens rotations
+// to column j, forms the new one and runs the convergence test
+// (KSPGMRESUpdateHessenberg, KSPConvergedDefault).
 constexpr int MAXPY_CHUNKS = 64;
+constexpr int MAXPY_SPAN = 2 * MAXPY_CHUNKS;   // chunks per CTA
 template <typename VT>
 __global__ void __launch_bounds__(ORTHO_THREADS)
 gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresState *st, GmresArrays ga)
@@ -515,56 +520,72 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
   constexpr int E = Chunk<VT>::E;
   __shared__ double hk[1024];
   __shared__ double sh[ORTHO_THREADS / 32];
-  __shared__ double qs[ORTHO_THREADS / MAXPY_CHUNKS][E][MAXPY_CHUNKS];
+  __shared__ double qs[ORTHO_THREADS / MAXPY_CHUNKS][E][MAXPY_SPAN];
   const int m = st->m;
-  for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[hidx(k, j, m)];
+  for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[hidx(k, j, m)] * ga.sigma[k];
   __syncthreads();
   VT *w = V + (int64_t)(j + 1) * ldv;
   const int lp = threadIdx.x % MAXPY_CHUNKS;
   const int quarter = threadIdx.x / MAXPY_CHUNKS;
-  const int64_t p = (int64_t)blockIdx.x * MAXPY_CHUNKS + lp;
-  double acc[E];
+  const int64_t p0 = (int64_t)blockIdx.x * MAXPY_SPAN + lp;
+  const int64_t p1 = p0 + MAXPY_CHUNKS;
+  double a0[E], a1[E];
 #pragma unroll
-  for (int e = 0; e < E; e++) acc[e] = 0.0;
-  if (p < nchunk) {
-    const VT *base = V + E * p;
+  for (int e = 0; e < E; e++) { a0[e] = 0.0; a1[e] = 0.0; }
+  // nchunk is a multiple of 16 (ldv is a multiple of 32 entries), so a CTA
+  // either owns both chunks of a thread or neither past the end
+  if (p1 < nchunk) {
+    const VT *b0 = V + E * p0;
+    const VT *b1 = V + E * p1;
     int k = quarter;
-    for (; k + 12 <= j; k += 16) {
-      double v0[E], v1[E], v2[E], v3[E];
-      Chunk<VT>::load(base + (int64_t)k * ldv, v0);
-      Chunk<VT>::load(base + (int64_t)(k + 4) * ldv, v1);
-      Chunk<VT>::load(base + (int64_t)(k + 8) * ldv, v2);
-      Chunk<VT>::load(base + (int64_t)(k + 12) * ldv, v3);
+    for (; k + 4 <= j; k += 8) {
+      double v0[E], v1[E], u0[E], u1[E];
+      Chunk<VT>::load(b0 + (int64_t)k * ldv, v0);
+      Chunk<VT>::load(b1 + (int64_t)k * ldv, u0);
+      Chunk<VT>::load(b0 + (int64_t)(k + 4) * ldv, v1);
+      Chunk<VT>::load(b1 + (int64_t)(k + 4) * ldv, u1);
 #pragma unroll
       for (int e = 0; e < E; e++) {
-        acc[e] = fma(hk[k], v0[e], acc[e]);
-        acc[e] = fma(hk[k + 4], v1[e], acc[e]);
-        acc[e] = fma(hk[k + 8], v2[e], acc[e]);
-        acc[e] = fma(hk[k + 12], v3[e], acc[e]);
+        a0[e] = fma(hk[k], v0[e], a0[e]);
+        a1[e] = fma(hk[k], u0[e], a1[e]);
+        a0[e] = fma(hk[k + 4], v1[e], a0[e]);
+        a1[e] = fma(hk[k + 4], u1[e], a1[e]);
       }
     }
     for (; k <= j; k += 4) {
-      double v0[E];
-      Chunk<VT>::load(base + (int64_t)k * ldv, v0);
+      double v0[E], u0[E];
+      Chunk<VT>::load(b0 + (int64_t)k * ldv, v0);
+      Chunk<VT>::load(b1 + (int64_t)k * ldv, u0);
 #pragma unroll
-      for (int e = 0; e < E; e++) acc[e] = fma(hk[k], v0[e], acc[e]);
+      for (int e = 0; e < E; e++) {
+        a0[e] = fma(hk[k], v0[e], a0[e]);
+        a1[e] = fma(hk[k], u0[e], a1[e]);
+      }
     }
   }
 #pragma unroll
-  for (int e = 0; e < E; e++) qs[quarter][e][lp] = acc[e];
+  for (int e = 0; e < E; e++) {
+    qs[quarter][e][lp] = a0[e];
+    qs[quarter][e][lp + MAXPY_CHUNKS] = a1[e];
+  }
   __syncthreads();
   double s = 0.0;
-  if (quarter == 0 && p < nchunk) {
-    double a[E];
-    Chunk<VT>::load(w + E * p, a);
+  // quarter q < 2 finishes chunk lp + q*MAXPY_CHUNKS
+  if (quarter < 2) {
+    const int c = lp + quarter * MAXPY_CHUNKS;
+    const int64_t p = (int64_t)blockIdx.x * MAXPY_SPAN + c;
+    if (p < nchunk) {
+      double a[E];
+      Chunk<VT>::load(w + E * p, a);
 #pragma unroll
-    for (int e = 0; e < E; e++) a[e] -= ((qs[0][e][lp] + qs[1][e][lp]) + (qs[2][e][lp] + qs[3][e][lp]));
-    Chunk<VT>::store(w + E * p, a);
-    // the norm is taken of the stored (possibly rounded) values
+      for (int e = 0; e < E; e++) a[e] -= ((qs[0][e][c] + qs[1][e][c]) + (qs[2][e][c] + qs[3][e][c]));
+      Chunk<VT>::store(w + E * p, a);
+      // the norm is taken of the stored (possibly rounded) values
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const double v = (double)(VT)a[e];
-      s = fma(v, v, s);
+      for (int e = 0; e < E; e++) {
+        const double v = (double)(VT)a[e];
+        s = fma(v, v, s);
+      }
     }
   }
   s = block_sum<ORTHO_THREADS>(s, sh);
@@ -585,6 +606,7 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
     if (threadIdx.x == 0) {
       const double tt = sqrt(t);
       st->tt = tt;
+      ga.sigma[it + 1] = (tt != 0.0) ? 1.0 / tt : 1.0;   // VecNormalize, applied lazily
       hc[it + 1] = tt;
       double hapbnd = fabs(tt / ga.grs[it]);
       if (hapbnd > 1.0e-30) hapbnd = 1.0e-30;
@@ -632,26 +654,6 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
   }
 }
 
-// V_{j+1} /= tt (VecNormalize), only if step j ran
-template <typename VT>
-__global__ void gmres_scale_next(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j,
-                                 const GmresState *__restrict__ st)
-{
-  if (st->it != j + 1) return;
-  const double tt = st->tt;
-  if (tt == 0.0) return;
-  constexpr int E = Chunk<VT>::E;
-  const double s = 1.0 / tt;
-  VT *w = V + (int64_t)(j + 1) * ldv;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nchunk; p += (int64_t)gridDim.x * blockDim.x) {
-    double a[E];
-    Chunk<VT>::load(w + E * p, a);
-#pragma unroll
-    for (int e = 0; e < E; e++) a[e] *= s;
-    Chunk<VT>::store(w + E * p, a);
-  }
-}
-
 // KSPGMRESBuildSoln back substitution, column-oriented: one CTA; for k from
 // the last column down, y_k = r_k / H(k,k), then r_i -= H(i,k) y_k for i < k.
 __global__ void __launch_bounds__(1024) gmres_backsub(GmresState *st, GmresArrays ga)
@@ -676,7 +678,7 @@ __global__ void __launch_bounds__(1024) gmres_backsub(GmresState *st, GmresArray
   }
 }
 
-// x += scale * sum_{k < it} y_k V_k  (x is FP64 whatever the basis type)
+// x += scale * sum_{k < it} y_k sigma_k V_k  (x is FP64 whatever the basis type)
 template <typename VT>
 __global__ void __launch_bounds__(ORTHO_THREADS)
 gmres_update_x(int64_t n, double *__restrict__ x, const VT *__restrict__ V, int64_t ldv,
@@ -685,7 +687,7 @@ gmres_update_x(int64_t n, double *__restrict__ x, const VT *__restrict__ V, int6
   __shared__ double yk[1024];
   const int it = st->it;
   if (it <= 0) return;
-  for (int k = threadIdx.x; k < it; k += blockDim.x) yk[k] = ga.y[k];
+  for (int k = threadIdx.x; k < it; k += blockDim.x) yk[k] = ga.y[k] * ga.sigma[k];
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
