@@ -23,8 +23,9 @@ EXPORTS = [
     "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual", "cfdgpu_residual_norm_noalloc",
     "cfdgpu_mpnn_create", "cfdgpu_mpnn_destroy", "cfdgpu_mpnn_num_params", "cfdgpu_mpnn_get_params",
     "cfdgpu_mpnn_set_params", "cfdgpu_mpnn_set_scales", "cfdgpu_mpnn_add_sample", "cfdgpu_mpnn_num_samples",
-    "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess",
+    "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess_mode", "cfdgpu_set_guess",
 ]
+GUESS = {"network": 1, "network_velocity": 2, "extrapolation": 4}
 KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
 
 OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV, ETOOBIG = 0, -1, -2, -3, -4, -5, -6, -7
@@ -58,7 +59,7 @@ class StepStats(ctypes.Structure):
                 ("ksp_reason", ctypes.c_int * MAX_NEWTON), ("refinements", ctypes.c_int * MAX_NEWTON),
                 ("ms_assembly", ctypes.c_double), ("ms_solver", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("guess_used", ctypes.c_int), ("guess_norm", ctypes.c_double), ("plain_norm", ctypes.c_double),
-                ("guess_alpha", ctypes.c_double)]
+                ("guess_alpha", ctypes.c_double), ("guess_alpha2", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         n = self.newton_iters
@@ -67,7 +68,8 @@ class StepStats(ctypes.Structure):
                 "ksp_its": list(self.ksp_its[:nsolve]), "ksp_reason": list(self.ksp_reason[:nsolve]),
                 "refinements": list(self.refinements[:nsolve]), "ms_assembly": self.ms_assembly,
                 "ms_solver": self.ms_solver, "ms_total": self.ms_total, "guess_used": bool(self.guess_used),
-                "guess_norm": self.guess_norm, "plain_norm": self.plain_norm, "guess_alpha": self.guess_alpha}
+                "guess_norm": self.guess_norm, "plain_norm": self.plain_norm, "guess_alpha": self.guess_alpha,
+                "guess_alpha2": self.guess_alpha2}
 
 
 class PatternInfo(ctypes.Structure):
@@ -124,6 +126,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_mpnn_train.argtypes = [vp, ip, ctypes.c_float, vp]
     L.cfdgpu_mpnn_predict.argtypes = [vp, vp, vp, vp]
     L.cfdgpu_set_guess.argtypes = [vp, vp]
+    L.cfdgpu_set_guess_mode.argtypes = [vp, vp, ip]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
     L.cfdgpu_set_profiling.argtypes = [vp, ip]
@@ -192,7 +195,8 @@ class Handle:
     def __init__(self, mesh, ctrl, restart: int = 50, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e4,
                  max_it: int = 10000, pc: str = "jacobi", precision: str = "fp64", inner_restart: int = 0,
                  inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
-                 newton_max_iter: int = 10, refine_rtol: float = 1e-10, newton_rtol: float = 0.0):
+                 newton_max_iter: int = 10, refine_rtol: float = 1e-10, newton_rtol: float = 0.0,
+                 guess: str = "constant"):
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()
@@ -210,6 +214,10 @@ class Handle:
             L.cfdgpu_destroy(self.h)
             self.h = ctypes.c_void_p()
             raise CfdGpuError(rc, msg)
+        if guess == "extrapolation":
+            self.set_guess_mode(("extrapolation",))
+        elif guess != "constant":
+            raise ValueError(f"guess must be 'constant' or 'extrapolation', not {guess!r}")
 
     def _check(self, rc: int):
         if rc != 0:
@@ -328,6 +336,13 @@ class Handle:
     def launch_count(self) -> int:
         return int(self._L.cfdgpu_launch_count(self.h))
 
+    def set_guess_mode(self, mode=()):
+        """Guess directions without a network (e.g. ("extrapolation",)); () = constant predictor."""
+        flags = 0
+        for k in mode:
+            flags |= GUESS[k]
+        self._check(self._L.cfdgpu_set_guess_mode(self.h, None, flags))
+
     def set_profiling(self, on: bool):
         self._check(self._L.cfdgpu_set_profiling(self.h, 1 if on else 0))
 
@@ -416,9 +431,13 @@ class Mpnn:
         self._check(self._L.cfdgpu_mpnn_predict(self.m, _ptr(a), _ptr(b), _ptr(d)))
         return d
 
-    def attach(self):
-        """Use this network as the handle's Newton initial guess."""
-        self._check(self._L.cfdgpu_set_guess(self.handle.h, self.m))
+    def attach(self, mode=("network", "extrapolation")):
+        """Use this network (and optionally the extrapolated increment) as the
+        handle's Newton initial guess."""
+        flags = 0
+        for k in mode:
+            flags |= GUESS[k]
+        self._check(self._L.cfdgpu_set_guess_mode(self.handle.h, self.m, flags))
 
     def detach(self):
         self._check(self._L.cfdgpu_set_guess(self.handle.h, None))

@@ -88,7 +88,9 @@ struct cfdgpu_handle {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // learned initial guess
   cfdgpu_mpnn *guess = nullptr;
-  double *guess_delta = nullptr, *rhs_plain = nullptr;
+  int guess_mode = 0;
+  double *guess_delta = nullptr, *rhs_plain = nullptr, *guess_dir2 = nullptr, *guess_res1 = nullptr,
+         *guess_res2 = nullptr;
   // per-kernel event timing
   bool prof = false;
   std::vector<cudaEvent_t> pev;          // pool of 2*PROF_POOL events
@@ -285,6 +287,23 @@ __global__ void k_round_f32(int64_t n4, const double *__restrict__ a, float *__r
     const double2 v = reinterpret_cast<const double2 *>(a)[2 * i + 1];
     reinterpret_cast<float4 *>(b)[i] = make_float4((float)u.x, (float)u.y, (float)v.x, (float)v.y);
   }
+}
+
+// zero dof d of every node
+__global__ void k_zero_dof(int nNode, int ndof, int d, double *__restrict__ v)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nNode) v[(int64_t)i * ndof + d] = 0.0;
+}
+
+// d = a - b on free dofs, 0 on prescribed ones
+__global__ void k_diff_free(int nNode, int ndof, const double *__restrict__ a, const double *__restrict__ b,
+                            const uint8_t *__restrict__ fixmask, double *__restrict__ d)
+{
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nNode * ndof) return;
+  const int node = (int)(t / ndof), dof = (int)(t % ndof);
+  d[t] = ((fixmask[node] >> dof) & 1u) ? 0.0 : a[t] - b[t];
 }
 
 // y = a*x + b*y
@@ -826,7 +845,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
   }
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
-  if ((rc = dalloc(h, &h->red_partial2, (size_t)2 * RED_BLOCKS))) return rc;
+  if ((rc = dalloc(h, &h->red_partial2, (size_t)5 * RED_BLOCKS))) return rc;
   if ((rc = dalloc(h, &h->red_counter, 1))) return rc;
   CK(cudaMemset(h->red_counter, 0, sizeof(unsigned int)));
   if ((rc = dalloc(h, &h->scalar, 8))) return rc;
@@ -886,42 +905,83 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     if ((rc = update_iter_step(h))) return rc;
     const bool want_K = !reuse || iter == 0;
     if ((rc = assemble(h, iter, want_K))) return rc;
-    if (iter == 0 && h->guess) {
-      // Network guess u_n + alpha*delta on the free dofs.  The iteration-0
-      // residual is affine in soln, F(u_n + alpha*delta) = F_A + alpha (F_B - F_A)
-      // with F_A at the constant predictor and F_B at alpha = 1, so alpha is
-      // chosen to minimise its norm; alpha <= 0 or no decrease keeps the
-      // constant predictor (the reference's guess) unchanged.
+    if (iter == 0 && (h->guess || (h->guess_mode & CFDGPU_GUESS_EXTRAPOLATION))) {
+      // Initial guess u_n + a1*d1 + a2*d2 on the free dofs, d1 the network's
+      // predicted increment (optionally velocity only), d2 the extrapolated
+      // increment u_n - u_{n-1}.  The iteration-0 residual is affine in the
+      // state, F(u_n + d) = F_A - K d, and K d_i = F_A - F(u_n + d_i), so the
+      // coefficients minimising ||F|| come from a 2x2 least-squares problem on
+      // the two residual differences.  No decrease keeps the constant
+      // predictor (the reference's guess) unchanged.
       double nplain = 0.0;
       if ((rc = norm2(h, h->rhs, &nplain))) return rc;
       CK(cudaMemcpyAsync(h->rhs_plain, h->rhs, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
-      if ((rc = cfdgpu::mpnn_predict_increment(h->guess, h->prev, h->prev2, h->guess_delta, h->stream))) {
-        h->err = "guess network failed";
-        return rc;
+      const bool use_net = h->guess && (h->guess_mode & (CFDGPU_GUESS_NETWORK | CFDGPU_GUESS_NETWORK_VELOCITY));
+      const bool use_ext = (h->guess_mode & CFDGPU_GUESS_EXTRAPOLATION) != 0;
+      double *dir[2] = {h->guess_delta, h->guess_dir2};
+      double *res[2] = {h->guess_res1, h->guess_res2};
+      int nd = 0;
+      if (use_net) {
+        if ((rc = cfdgpu::mpnn_predict_increment(h->guess, h->prev, h->prev2, h->guess_delta, h->stream))) {
+          h->err = "guess network failed";
+          return rc;
+        }
+        if (!(h->guess_mode & CFDGPU_GUESS_NETWORK)) {
+          k_zero_dof<<<grid_for(h->nNode), 256, 0, h->stream>>>(h->nNode, h->ndof, h->ndof - 1, h->guess_delta);
+          LAUNCHED(h);
+        }
+        dir[nd++] = h->guess_delta;
       }
-      k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0, h->guess_delta, h->soln);
+      if (use_ext) {
+        double *d2 = (nd == 0) ? h->guess_delta : h->guess_dir2;
+        k_diff_free<<<grid_for(h->n), 256, 0, h->stream>>>(h->nNode, h->ndof, h->prev, h->prev2, h->fixmask, d2);
+        LAUNCHED(h);
+        dir[nd++] = d2;
+      }
+      for (int q = 0; q < nd; q++) {
+        CK(cudaMemcpyAsync(h->soln, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+        k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0, dir[q], h->soln);
+        LAUNCHED(h);
+        if ((rc = update_iter_step(h))) return rc;
+        if ((rc = assemble(h, 0, false))) return rc;
+        CK(cudaMemcpyAsync(res[q], h->rhs, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+      }
+      minres_dots2<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(h->n, h->rhs_plain, res[0], nd > 1 ? res[1] : res[0],
+                                                             h->red_partial2, h->red_counter, h->scalar + 2);
       LAUNCHED(h);
-      if ((rc = update_iter_step(h))) return rc;
-      if ((rc = assemble(h, 0, false))) return rc;
-      minres_dots<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(h->n, h->rhs_plain, h->rhs, h->red_partial2, h->red_counter,
-                                                            h->scalar + 2);
-      LAUNCHED(h);
-      CK(cudaMemcpyAsync(h->h_scalar + 2, h->scalar + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(h->h_scalar + 2, h->scalar + 2, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       CK(cudaStreamSynchronize(h->stream));
-      const double num = h->h_scalar[2], den = h->h_scalar[3];
-      const double alpha = (den > 0.0 && num > 0.0) ? num / den : 0.0;
-      const double nres2 = nplain * nplain - (den > 0.0 ? num * num / den : 0.0);
-      const double nguess = std::sqrt(std::max(nres2, 0.0));
+      const double r1 = h->h_scalar[2], r2 = h->h_scalar[3], g11 = h->h_scalar[4], g12 = h->h_scalar[5],
+                   g22 = h->h_scalar[6];
+      double a1 = 0.0, a2 = 0.0;
+      const double det = g11 * g22 - g12 * g12;
+      if (nd > 1 && det > 1e-12 * g11 * g22) {
+        a1 = (r1 * g22 - r2 * g12) / det;
+        a2 = (g11 * r2 - g12 * r1) / det;
+      } else if (g11 > 0.0) {
+        a1 = r1 / g11;
+      }
+      const double decrease = a1 * r1 + (nd > 1 ? a2 * r2 : 0.0);   // ||F_A||^2 - ||F||^2
+      const double nguess = std::sqrt(std::max(nplain * nplain - decrease, 0.0));
       stats->plain_norm = nplain;
-      stats->guess_norm = (alpha > 0.0) ? nguess : nplain;
-      // soln = u_n + alpha * delta, rhs = (1 - alpha) F_A + alpha F_B
+      stats->guess_norm = nplain;
       CK(cudaMemcpyAsync(h->soln, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
-      if (alpha > 0.0 && nguess < nplain) {
+      if (decrease > 0.0 && nguess < nplain) {
         stats->guess_used = 1;
-        stats->guess_alpha = alpha;
-        k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, alpha, h->guess_delta, h->soln);
-        k_lincomb<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0 - alpha, h->rhs_plain, alpha, h->rhs);
+        stats->guess_alpha = a1;
+        stats->guess_alpha2 = (nd > 1) ? a2 : 0.0;
+        stats->guess_norm = nguess;
+        // soln = u_n + a1 d1 + a2 d2 ; rhs = (1 - a1 - a2) F_A + a1 F_1 + a2 F_2
+        k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, a1, dir[0], h->soln);
+        k_lincomb<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, a1, res[0], 0.0, h->rhs);
         h->launches += 2;
+        if (nd > 1) {
+          k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, a2, dir[1], h->soln);
+          k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, a2, res[1], h->rhs);
+          h->launches += 2;
+        }
+        k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0 - a1 - (nd > 1 ? a2 : 0.0), h->rhs_plain, h->rhs);
+        LAUNCHED(h);
       } else {
         CK(cudaMemcpyAsync(h->rhs, h->rhs_plain, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
       }
@@ -977,13 +1037,23 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
 
 int cfdgpu_set_guess(cfdgpu_handle *h, cfdgpu_mpnn *m)
 {
+  return cfdgpu_set_guess_mode(h, m, m ? (CFDGPU_GUESS_NETWORK | CFDGPU_GUESS_EXTRAPOLATION) : 0);
+}
+
+int cfdgpu_set_guess_mode(cfdgpu_handle *h, cfdgpu_mpnn *m, int mode)
+{
   if (!h) return CFDGPU_EINVAL;
-  if (m && !h->guess_delta) {
+  if (mode && !h->guess_delta) {
     int rc;
     if ((rc = dalloc(h, &h->guess_delta, (size_t)h->n))) return rc;
     if ((rc = dalloc(h, &h->rhs_plain, (size_t)h->n))) return rc;
+    if ((rc = dalloc(h, &h->guess_dir2, (size_t)h->n))) return rc;
+    if ((rc = dalloc(h, &h->guess_res1, (size_t)h->n))) return rc;
+    if ((rc = dalloc(h, &h->guess_res2, (size_t)h->n))) return rc;
   }
+  if (!m) mode &= ~(CFDGPU_GUESS_NETWORK | CFDGPU_GUESS_NETWORK_VELOCITY);
   h->guess = m;
+  h->guess_mode = mode;
   return 0;
 }
 

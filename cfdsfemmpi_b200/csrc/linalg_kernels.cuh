@@ -391,6 +391,36 @@ minres_dots(int64_t n, const double *__restrict__ a, const double *__restrict__ 
   }
 }
 
+// Gram data of two residual differences k_i = a - b_i (deterministic):
+// out = [<a,k1>, <a,k2>, <k1,k1>, <k1,k2>, <k2,k2>]; partial holds 5*gridDim.x
+__global__ void __launch_bounds__(RED_THREADS)
+minres_dots2(int64_t n, const double *__restrict__ a, const double *__restrict__ b1, const double *__restrict__ b2,
+             double *__restrict__ partial, unsigned int *counter, double *__restrict__ out)
+{
+  __shared__ double sh[RED_THREADS / 32];
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {
+    const double k1 = a[i] - b1[i], k2 = a[i] - b2[i];
+    s[0] = fma(a[i], k1, s[0]);
+    s[1] = fma(a[i], k2, s[1]);
+    s[2] = fma(k1, k1, s[2]);
+    s[3] = fma(k1, k2, s[3]);
+    s[4] = fma(k2, k2, s[4]);
+  }
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    const double t = block_sum<RED_THREADS>(s[q], sh);
+    if (threadIdx.x == 0) partial[5 * blockIdx.x + q] = t;
+  }
+  if (last_block(counter, gridDim.x)) {
+    if (threadIdx.x < 5) {
+      double t = 0.0;
+      for (unsigned int k = 0; k < gridDim.x; k++) t += partial[5 * k + threadIdx.x];
+      out[threadIdx.x] = t;
+    }
+  }
+}
+
 // GMRES cycle start: res = ||V0||, convergence test at its, v0scale.
 template <typename VT>
 __global__ void __launch_bounds__(RED_THREADS)

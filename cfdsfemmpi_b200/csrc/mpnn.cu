@@ -237,14 +237,22 @@ __global__ void k_features(int N, int ndof, int ndim, const double *__restrict__
   for (int c = 0; c < FIN; c++) X[(int64_t)i * FIN + c] = __float2bfloat16(f[c]);
 }
 
-__global__ void k_targets(int N, int ndof, const double *__restrict__ un, const double *__restrict__ unp1, float t0,
-                          float t1, float t2, float t3, float *__restrict__ T)
+// target: the correction over linear extrapolation, u_{n+1} - 2 u_n + u_{n-1}, scaled
+__global__ void k_targets(int N, int ndof, const double *__restrict__ unm1, const double *__restrict__ un,
+                          const double *__restrict__ unp1, float t0, float t1, float t2, float t3,
+                          float *__restrict__ T)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const float ts[4] = {t0, t1, t2, t3};
-  for (int c = 0; c < FOUT; c++)
-    T[(int64_t)i * FOUT + c] = (c < ndof) ? (float)((unp1[(int64_t)i * ndof + c] - un[(int64_t)i * ndof + c]) / ts[c]) : 0.f;
+  for (int c = 0; c < FOUT; c++) {
+    float v = 0.f;
+    if (c < ndof) {
+      const int64_t k = (int64_t)i * ndof + c;
+      v = (float)(((unp1[k] - un[k]) - (un[k] - unm1[k])) / ts[c]);
+    }
+    T[(int64_t)i * FOUT + c] = v;
+  }
 }
 
 __global__ void k_mask(int N, int ndof, const uint8_t *__restrict__ fixmask, float *__restrict__ mask)
@@ -394,14 +402,18 @@ __global__ void k_wcopy(int K, int NO, const float *__restrict__ W, bf16 *__rest
   Wtb[o * K + k] = b;
 }
 
+// predicted increment = extrapolated increment u_n - u_{n-1} + learned correction
 __global__ void k_write_delta(int N, int ndof, const float *__restrict__ y, float t0, float t1, float t2, float t3,
+                              const double *__restrict__ un, const double *__restrict__ unm1,
                               const uint8_t *__restrict__ fixmask, double *__restrict__ delta)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const float ts[4] = {t0, t1, t2, t3};
-  for (int c = 0; c < ndof; c++)
-    delta[(int64_t)i * ndof + c] = ((fixmask[i] >> c) & 1u) ? 0.0 : (double)y[(int64_t)i * FOUT + c] * (double)ts[c];
+  for (int c = 0; c < ndof; c++) {
+    const int64_t k = (int64_t)i * ndof + c;
+    delta[k] = ((fixmask[i] >> c) & 1u) ? 0.0 : (un[k] - unm1[k]) + (double)y[(int64_t)i * FOUT + c] * (double)ts[c];
+  }
 }
 
 inline int grid1(int64_t n, int bs = 256) { return (int)std::min<int64_t>((n + bs - 1) / bs, 148 * 32); }
@@ -518,7 +530,8 @@ int mpnn_predict_increment(cfdgpu_mpnn *m, const double *u_n, const double *u_nm
   rc = forward(m, m->X);
   if (rc) return rc;
   k_write_delta<<<(N + 255) / 256, 256, 0, m->g.stream>>>(N, m->g.ndof, m->Y, m->out_scale[0], m->out_scale[1],
-                                                          m->out_scale[2], m->out_scale[3], m->g.fixmask, delta);
+                                                          m->out_scale[2], m->out_scale[3], u_n, u_nm1,
+                                                          m->g.fixmask, delta);
   return cudaGetLastError() == cudaSuccess ? 0 : CFDGPU_ECUDA;
 }
 
@@ -642,8 +655,9 @@ int cfdgpu_mpnn_add_sample(cfdgpu_mpnn *m, const double *u_nm1, const double *u_
   cudaMemcpyAsync(tmp + n, u_n, sizeof(double) * n, cudaMemcpyHostToDevice, m->g.stream);
   cudaMemcpyAsync(tmp + 2 * n, u_np1, sizeof(double) * n, cudaMemcpyHostToDevice, m->g.stream);
   rc = sample_features(m, tmp, tmp + n, X);
-  k_targets<<<(m->N + 255) / 256, 256, 0, m->g.stream>>>(m->N, m->g.ndof, tmp + n, tmp + 2 * n, m->out_scale[0],
-                                                         m->out_scale[1], m->out_scale[2], m->out_scale[3], T);
+  k_targets<<<(m->N + 255) / 256, 256, 0, m->g.stream>>>(m->N, m->g.ndof, tmp, tmp + n, tmp + 2 * n,
+                                                         m->out_scale[0], m->out_scale[1], m->out_scale[2],
+                                                         m->out_scale[3], T);
   cudaStreamSynchronize(m->g.stream);
   cudaFree(tmp);
   if (rc || cudaGetLastError() != cudaSuccess) return CFDGPU_ECUDA;

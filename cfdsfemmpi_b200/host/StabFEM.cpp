@@ -184,7 +184,14 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
     std::cerr << " cfdgpu_create failed: " << cfdgpu_last_error(gpu) << std::endl;
     return rc;
   }
-  return 0;
+  const std::string guess = get("-gpu_guess", "constant");
+  if (guess == "extrapolation") {
+    rc = cfdgpu_set_guess_mode(gpu, nullptr, CFDGPU_GUESS_EXTRAPOLATION);
+  } else if (guess != "constant") {
+    std::cerr << " -gpu_guess must be constant or extrapolation" << std::endl;
+    rc = CFDGPU_EINVAL;
+  }
+  return rc;
 }
 
 // Time loop of StabFEM::solveFullyImplicit (src/base/StabFEM2.cpp:593-832)

@@ -13,6 +13,9 @@ plus this library's own keys:
 
   -gpu_precision fp64|mixed   -gpu_inner_restart m    -gpu_inner_rtol r
   -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_newton_rtol r
+  -gpu_guess constant|extrapolation   (Newton initial guess; constant = the
+                                       reference's, extrapolation = u_n plus
+                                       the min-residual multiple of u_n - u_{n-1})
 
 The GPU library has no direct solver.  ``-ksp_type preonly -pc_type lu`` (the
 reference's shipped tests) is served by GMRES with point-block Jacobi at a
@@ -73,6 +76,8 @@ def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
         kw["refine_rtol"] = float(opts["-gpu_refine_rtol"])
     if "-gpu_newton_rtol" in opts:
         kw["newton_rtol"] = float(opts["-gpu_newton_rtol"])
+    if "-gpu_guess" in opts:
+        kw["guess"] = opts["-gpu_guess"].lower()
     kw["_notes"] = notes
     return kw
 
@@ -140,6 +145,8 @@ class StabFEM:
     def solver_description(self) -> str:
         k = self.solver_kw
         s = f"GMRES({k['restart']}) pc={k['pc']} rtol={k['rtol']:g} max_it={k['max_it']} precision={k['precision']}"
+        if k.get("guess", "constant") != "constant":
+            s += f" guess={k['guess']}"
         if k.get("_notes"):
             s += " [" + "; ".join(k["_notes"]) + "]"
         return s

@@ -6,13 +6,16 @@ csrc/mpnn.cu; this module drives it:
 * ``collect_trajectory`` runs the plain solver (the library's own time step)
   from rest and keeps the nodal solution after every step;
 * ``fit_scales`` picks per-component scales for u_n, u_n - u_{n-1} and the
-  increment u_{n+1} - u_n from that trajectory;
+  network's target, the correction over linear extrapolation
+  u_{n+1} - 2 u_n + u_{n-1}, from that trajectory;
 * ``train_guess`` adds the (u_{n-1}, u_n, u_{n+1}) samples and runs Adam.
 
-``Mpnn.attach()`` then makes ``cfdgpu_step`` start Newton from u_n + the
-predicted increment whenever that lowers the iteration-0 residual, and from
-the reference's constant predictor otherwise.  The converged answer always
-comes from the unchanged Newton-GMRES loop.
+``Mpnn.attach()`` then makes ``cfdgpu_step`` start Newton from
+u_n + a1*(predicted increment) + a2*(u_n - u_{n-1}), the coefficients
+minimising the iteration-0 residual exactly (the residual is affine in the
+state), whenever that lowers it, and from the reference's constant
+predictor otherwise.  The converged answer always comes from the unchanged
+Newton-GMRES loop.
 """
 from __future__ import annotations
 
@@ -38,14 +41,19 @@ def collect_trajectory(mesh, ctrl, steps: int, **solver_kw) -> Tuple[List[np.nda
 
 
 def fit_scales(traj: List[np.ndarray], ndof: int, floor: float = 1e-6) -> Tuple[np.ndarray, np.ndarray]:
-    """Root-mean-square per component of u_n, u_n - u_{n-1} and u_{n+1} - u_n."""
-    U = np.stack(traj[1:]).reshape(len(traj) - 1, -1, ndof)
-    D = np.diff(np.stack(traj), axis=0).reshape(len(traj) - 1, -1, ndof)
-    su = np.sqrt(np.mean(U ** 2, axis=(0, 1)))
-    sd = np.sqrt(np.mean(D ** 2, axis=(0, 1)))
-    su = np.maximum(su, floor)
-    sd = np.maximum(sd, floor)
-    return np.concatenate([su, sd]).astype(np.float32), sd.astype(np.float32)
+    """Root-mean-square per component of u_n, u_n - u_{n-1} (features) and of
+    u_{n+1} - 2 u_n + u_{n-1} (target)."""
+    S = np.stack(traj)
+    U = S[1:].reshape(len(traj) - 1, -1, ndof)
+    D = np.diff(S, axis=0).reshape(len(traj) - 1, -1, ndof)
+    su = np.maximum(np.sqrt(np.mean(U ** 2, axis=(0, 1))), floor)
+    sd = np.maximum(np.sqrt(np.mean(D ** 2, axis=(0, 1))), floor)
+    if len(traj) >= 3:
+        D2 = np.diff(S, n=2, axis=0).reshape(len(traj) - 2, -1, ndof)
+        s2 = np.maximum(np.sqrt(np.mean(D2 ** 2, axis=(0, 1))), floor * 1e-3)
+    else:
+        s2 = sd
+    return np.concatenate([su, sd]).astype(np.float32), s2.astype(np.float32)
 
 
 def train_guess(handle: Handle, traj: List[np.ndarray], iters: int = 2000, lr: float = 2e-3, seed: int = 0,

@@ -108,9 +108,10 @@ typedef struct cfdgpu_step_stats {
   int ksp_reason[CFDGPU_MAX_NEWTON];    /* PETSc-style KSPConvergedReason per solve */
   int refinements[CFDGPU_MAX_NEWTON];   /* mixed mode: outer refinement passes per solve */
   double ms_assembly, ms_solver, ms_total;
-  int guess_used;                       /* 1: the network's initial guess was kept */
-  double guess_norm, plain_norm;        /* iteration-0 residual norms of both guesses (when a model is set) */
-  double guess_alpha;                   /* step length along the predicted increment (0: constant predictor) */
+  int guess_used;                       /* 1: the combined initial guess was kept */
+  double guess_norm, plain_norm;        /* iteration-0 residual norms of both guesses (when a guess mode is set) */
+  double guess_alpha;                   /* coefficient of the first guess direction (0: constant predictor) */
+  double guess_alpha2;                  /* coefficient of the second direction (0 when only one is set) */
 } cfdgpu_step_stats;
 
 typedef struct cfdgpu_handle cfdgpu_handle;
@@ -228,7 +229,9 @@ int64_t cfdgpu_launch_count(cfdgpu_handle *h);
 /* ---- learned Newton initial guess ------------------------------------
  * A message-passing network over the handle's node graph (hidden width 64,
  * three residual mean-aggregation layers) maps [u_n, u_n - u_{n-1}, X] to the
- * next-step increment.  Training and inference run on the device with the
+ * correction of the next-step increment over linear extrapolation,
+ * u_{n+1} - 2 u_n + u_{n-1}; the predicted increment is u_n - u_{n-1} plus
+ * that correction.  Training and inference run on the device with the
  * library's own kernels (BF16 tensor-core GEMMs, FP32 accumulation, FP32
  * Adam).  No counterpart in the reference: its Newton loop starts from the
  * previous step's solution (src/base/StabFEM2.cpp:654, SolutionData.cpp:64-78). */
@@ -238,8 +241,8 @@ int cfdgpu_mpnn_destroy(cfdgpu_mpnn *m);
 int cfdgpu_mpnn_num_params(cfdgpu_mpnn *m);
 int cfdgpu_mpnn_get_params(cfdgpu_mpnn *m, float *p);
 int cfdgpu_mpnn_set_params(cfdgpu_mpnn *m, const float *p);
-/* feature scales for u_n and u_n - u_{n-1} (2*ndof values) and target
- * scales (ndof values); set before adding samples */
+/* feature scales for u_n and u_n - u_{n-1} (2*ndof values) and scales of the
+ * correction target (ndof values); set before adding samples */
 int cfdgpu_mpnn_set_scales(cfdgpu_mpnn *m, const float *in_scale, const float *out_scale);
 /* one training sample (host arrays of nNode*ndof): u_{n-1}, u_n, u_{n+1} */
 int cfdgpu_mpnn_add_sample(cfdgpu_mpnn *m, const double *u_nm1, const double *u_n, const double *u_np1);
@@ -250,12 +253,18 @@ int cfdgpu_mpnn_loss_grad(cfdgpu_mpnn *m, int sample, float *loss, float *grad);
 int cfdgpu_mpnn_train(cfdgpu_mpnn *m, int iters, float lr, float *loss_out);
 /* predicted increment (host arrays; zero at prescribed dofs) */
 int cfdgpu_mpnn_predict(cfdgpu_mpnn *m, const double *u_nm1, const double *u_n, double *delta);
-/* use the network as the Newton initial guess of cfdgpu_step (NULL: the
- * reference's constant predictor).  Each step evaluates the iteration-0
- * residual at u_n and at u_n + delta; the residual is affine in the state, so
- * the step length alpha minimising ||F(u_n + alpha*delta)|| is exact.  The
- * network's guess is kept only if alpha > 0 lowers the residual
- * (stats->guess_used); otherwise the step runs from the constant predictor. */
+/* Initial-guess directions for cfdgpu_step (bit flags). */
+#define CFDGPU_GUESS_NETWORK 1            /* the network's predicted increment */
+#define CFDGPU_GUESS_NETWORK_VELOCITY 2   /* the same, velocity dofs only */
+#define CFDGPU_GUESS_EXTRAPOLATION 4      /* u_n - u_{n-1} (linear extrapolation) */
+/* Newton initial guess of cfdgpu_step: u_n + a1*d1 + a2*d2 over the selected
+ * directions (at most two).  The iteration-0 residual is affine in the state,
+ * so one residual evaluation per direction gives the exact minimiser of
+ * ||F(u_n + a1 d1 + a2 d2)||; it is used only if it lowers the residual
+ * (stats->guess_used), otherwise the step runs from the reference's constant
+ * predictor.  mode 0 (or m NULL with network bits) = constant predictor. */
+int cfdgpu_set_guess_mode(cfdgpu_handle *h, cfdgpu_mpnn *m, int mode);
+/* cfdgpu_set_guess_mode(h, m, NETWORK | EXTRAPOLATION), or mode 0 for m = NULL */
 int cfdgpu_set_guess(cfdgpu_handle *h, cfdgpu_mpnn *m);
 
 /* Per-kernel device timing with CUDA events on the handle's stream (off by

@@ -59,10 +59,11 @@ def features(u_nm1, u_n, coords, ndof, ndim, in_scale):
     return bf16(f)
 
 
-def targets(u_n, u_np1, ndof, out_scale):
+def targets(u_nm1, u_n, u_np1, ndof, out_scale):
+    """Scaled correction over linear extrapolation, u_{n+1} - 2 u_n + u_{n-1}."""
     N = u_n.size // ndof
     t = np.zeros((N, FOUT), np.float32)
-    d = (u_np1 - u_n).reshape(N, ndof)
+    d = ((u_np1 - u_n) - (u_n - u_nm1)).reshape(N, ndof)
     for c in range(ndof):
         t[:, c] = (d[:, c] / np.float64(np.float32(out_scale[c]))).astype(np.float32)
     return t
