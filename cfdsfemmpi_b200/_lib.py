@@ -26,6 +26,7 @@ EXPORTS = [
     "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess_mode", "cfdgpu_set_guess",
 ]
 GUESS = {"network": 1, "network_velocity": 2, "extrapolation": 4}
+FORM = {"semi_implicit": 0, "fully_implicit": 1}
 KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
 
 OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV, ETOOBIG = 0, -1, -2, -3, -4, -5, -6, -7
@@ -50,7 +51,8 @@ class SolverOpts(ctypes.Structure):
     _fields_ = [("restart", ctypes.c_int), ("rtol", ctypes.c_double), ("atol", ctypes.c_double),
                 ("dtol", ctypes.c_double), ("max_it", ctypes.c_int), ("pc_type", ctypes.c_int),
                 ("precision", ctypes.c_int), ("inner_restart", ctypes.c_int), ("inner_rtol", ctypes.c_double),
-                ("reuse_tangent", ctypes.c_int), ("refine_rtol", ctypes.c_double), ("newton_rtol", ctypes.c_double)]
+                ("reuse_tangent", ctypes.c_int), ("refine_rtol", ctypes.c_double), ("newton_rtol", ctypes.c_double),
+                ("formulation", ctypes.c_int)]
 
 
 class StepStats(ctypes.Structure):
@@ -196,7 +198,7 @@ class Handle:
                  max_it: int = 10000, pc: str = "jacobi", precision: str = "fp64", inner_restart: int = 0,
                  inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
                  newton_max_iter: int = 10, refine_rtol: float = 1e-10, newton_rtol: float = 0.0,
-                 guess: str = "constant"):
+                 guess: str = "constant", formulation: str = "semi_implicit"):
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()
@@ -207,7 +209,7 @@ class Handle:
         c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
                     ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
         o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
-                       1 if reuse_tangent else 0, refine_rtol, newton_rtol)
+                       1 if reuse_tangent else 0, refine_rtol, newton_rtol, FORM[formulation])
         rc = L.cfdgpu_create(ctypes.byref(m), ctypes.byref(c), ctypes.byref(o), ctypes.byref(self.h))
         if rc != 0:
             msg = L.cfdgpu_last_error(self.h).decode() if self.h else "create failed"

@@ -330,7 +330,7 @@ static inline int grid_for(int64_t n, int bs = 256, int cap = 148 * 16)
 // ---------------------------------------------------------------------------
 // element launches
 
-template <int ET, int MODE, bool LIFT>
+template <int ET, int MODE, bool LIFT, int FORM>
 static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, double *outK, double *outF)
 {
   constexpr int GS = ElemTraits<ET>::GS;
@@ -349,11 +349,11 @@ static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, doub
   P.stab0 = h->ctrl.stab[0]; P.stab1 = h->ctrl.stab[1]; P.stab2 = h->ctrl.stab[2];
   if (h->mixed && MODE != MODE_EXPORT) {
     // FP64 arithmetic, FP32 storage of the tangent blocks
-    element_kernel<ET, double, float, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+    element_kernel<ET, double, float, MODE, LIFT, GROUPS, FORM><<<grid, GS * GROUPS, 0, h->stream>>>(
         elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr32,
         h->rhs, outK, outF, h->negjac);
   } else {
-    element_kernel<ET, double, double, MODE, LIFT, GROUPS><<<grid, GS * GROUPS, 0, h->stream>>>(
+    element_kernel<ET, double, double, MODE, LIFT, GROUPS, FORM><<<grid, GS * GROUPS, 0, h->stream>>>(
         elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
         h->rhs, outK, outF, h->negjac);
   }
@@ -362,15 +362,23 @@ static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, doub
   return check_launch(h, "element_kernel");
 }
 
+template <int MODE, bool LIFT, int FORM>
+static int launch_elements_form(cfdgpu_handle *h, const int32_t *elems, int nel, double *outK, double *outF)
+{
+  switch (h->et) {
+    case CFDGPU_HEX8: return launch_elements<CFDGPU_HEX8, MODE, LIFT, FORM>(h, elems, nel, outK, outF);
+    case CFDGPU_TET4: return launch_elements<CFDGPU_TET4, MODE, LIFT, FORM>(h, elems, nel, outK, outF);
+    case CFDGPU_QUAD4: return launch_elements<CFDGPU_QUAD4, MODE, LIFT, FORM>(h, elems, nel, outK, outF);
+    default: return launch_elements<CFDGPU_TRI3, MODE, LIFT, FORM>(h, elems, nel, outK, outF);
+  }
+}
+
 template <int MODE, bool LIFT>
 static int launch_elements_et(cfdgpu_handle *h, const int32_t *elems, int nel, double *outK, double *outF)
 {
-  switch (h->et) {
-    case CFDGPU_HEX8: return launch_elements<CFDGPU_HEX8, MODE, LIFT>(h, elems, nel, outK, outF);
-    case CFDGPU_TET4: return launch_elements<CFDGPU_TET4, MODE, LIFT>(h, elems, nel, outK, outF);
-    case CFDGPU_QUAD4: return launch_elements<CFDGPU_QUAD4, MODE, LIFT>(h, elems, nel, outK, outF);
-    default: return launch_elements<CFDGPU_TRI3, MODE, LIFT>(h, elems, nel, outK, outF);
-  }
+  if (h->opts.formulation == CFDGPU_FORM_FULLY_IMPLICIT)
+    return launch_elements_form<MODE, LIFT, FORM_FULLY_IMPLICIT>(h, elems, nel, outK, outF);
+  return launch_elements_form<MODE, LIFT, FORM_SEMI_IMPLICIT>(h, elems, nel, outK, outF);
 }
 
 // Assembly of one Newton iteration: rhs (and the tangent when want_K),
@@ -756,6 +764,10 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   if (h->opts.restart <= 0) h->opts.restart = 30;
   if (h->opts.restart > 1000) { h->err = "restart > 1000 is not supported"; return CFDGPU_EINVAL; }
   if (h->opts.max_it <= 0) h->opts.max_it = 10000;
+  if (h->opts.formulation != CFDGPU_FORM_SEMI_IMPLICIT && h->opts.formulation != CFDGPU_FORM_FULLY_IMPLICIT) {
+    h->err = "unknown element formulation";
+    return CFDGPU_EINVAL;
+  }
   if (h->ctrl.newton_max_iter <= 0) h->ctrl.newton_max_iter = 10;
   if (h->ctrl.newton_max_iter > CFDGPU_MAX_NEWTON) h->ctrl.newton_max_iter = CFDGPU_MAX_NEWTON;
   h->m = h->opts.restart;
@@ -898,7 +910,9 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     if ((rc = check_launch(h, "apply_bc"))) return rc;
   }
   const int nfix = (int)h->topo.fixed_dofs.size();
-  const bool reuse = h->opts.reuse_tangent != 0;
+  // the semi-implicit tangent depends only on solnPrev: one assembly per step;
+  // the fully-implicit tangent depends on the iterate: one per iteration
+  const bool reuse = h->opts.reuse_tangent != 0 && h->opts.formulation == CFDGPU_FORM_SEMI_IMPLICIT;
   double ms_asm = 0.0, ms_sol = 0.0;
   for (int iter = 0; iter < h->ctrl.newton_max_iter; iter++) {
     auto ta = std::chrono::steady_clock::now();
@@ -986,6 +1000,23 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
         CK(cudaMemcpyAsync(h->rhs, h->rhs_plain, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
       }
       if ((rc = update_iter_step(h))) return rc;
+      if (!reuse && stats->guess_used) {
+        // fully implicit: the residual is not affine and the tangent moves
+        // with the state, so the chosen guess is re-assembled and kept only
+        // if its true residual is lower
+        if ((rc = assemble(h, 0, true))) return rc;
+        double ntrue = 0.0;
+        if ((rc = norm2(h, h->rhs, &ntrue))) return rc;
+        stats->guess_norm = ntrue;
+        if (!(ntrue < nplain)) {
+          stats->guess_used = 0;
+          stats->guess_alpha = stats->guess_alpha2 = 0.0;
+          stats->guess_norm = nplain;
+          CK(cudaMemcpyAsync(h->soln, h->prev, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream));
+          if ((rc = update_iter_step(h))) return rc;
+          if ((rc = assemble(h, 0, true))) return rc;
+        }
+      }
     }
     if (iter == 0 && nfix) {
       k_dirichlet_update<<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->fixed_dofs, h->dbc_mult, h->applied, h->soln);

@@ -15,12 +15,19 @@
 //      no node, so a launch per colour is race-free and every matrix entry
 //      receives its contributions in the same order on every run.
 //
-// The arithmetic follows the active "semi-implicit type B" element routines
-// of the reference (file:line within the reference project):
+// FORM_SEMI_IMPLICIT follows the active "semi-implicit type B" element
+// routines of the reference (file:line within the reference project):
 //   quad4 src/base/LagrangeElem2DNavierStokesQuad4Node.cpp:683-970
 //   tri3  src/base/LagrangeElem2DNavierStokesTria3Node.cpp:683-968
 //   hex8  src/base/LagrangeElem3DNavierStokesHexa8Node.cpp:764-1074
 //   tet4  src/base/LagrangeElem3DNavierStokesTetra4Node.cpp:769-1078
+// FORM_FULLY_IMPLICIT follows the reference's commented-out "Fully-implicit
+// formulation" routines (quad4 :117-396, tri3 :117-396, hex8 :109-432, tet4
+// :115-438 of the same files): convection grad(u) u with its Newton
+// linearisation, SUPG weight on the current velocity with its derivative,
+// PSPG, LSIC in 3D, no sign-flipped rows, CI 10 (hex8) or 4; the 2D and 3D
+// texts differ (2D: SUPG without rho, af on the pressure column; 3D: SUPG
+// with rho, no af on the pressure column) and are kept as written.
 // with prepareElemData (basis, w*detJ, charlen) recomputed from coordinates
 // instead of stored, the basis of src/base/BasisFunctionsLagrange.cpp (hexa
 // p=1 derivative table as the reference writes it, :1053-1078), quadrature of
@@ -139,7 +146,7 @@ struct ElemSmem {
   double dvol[NGP];
   double vP[NGP][NDIM];
   double gP[NGP][NDIM][NDIM];
-  double tau0[NGP], tau1[NGP];
+  double tau0[NGP], tau1[NGP], tau2[NGP];
   double res2[NGP][NDIM];
   double stress[NGP][NDIM][NDIM];
   double rStab[NGP][NDIM];
@@ -149,11 +156,13 @@ struct ElemSmem {
 };
 
 enum { MODE_ASSEMBLE = 0, MODE_RESIDUAL = 1, MODE_EXPORT = 2 };
+enum { FORM_SEMI_IMPLICIT = 0, FORM_FULLY_IMPLICIT = 1 };
 
 // CT: arithmetic type of the tangent accumulation; KST: stored BSR type.
 // MODE_ASSEMBLE: K and F into the BSR/RHS (LIFT adds the iteration-0 lifting);
 // MODE_RESIDUAL: F only; MODE_EXPORT: raw K_e/F_e into dense per-element output.
-template <int ET, typename CT, typename KST, int MODE, bool LIFT, int GROUPS>
+// FORM: FORM_SEMI_IMPLICIT or FORM_FULLY_IMPLICIT.
+template <int ET, typename CT, typename KST, int MODE, bool LIFT, int GROUPS, int FORM>
 __global__ void __launch_bounds__(ElemTraits<ET>::GS * GROUPS)
 element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__restrict__ conn,
                const double *__restrict__ coords, const double *__restrict__ solnPrev,
@@ -165,6 +174,10 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
   using T = ElemTraits<ET>;
   constexpr int NDIM = T::NDIM, NPE = T::NPE, NGP = T::NGP, GS = T::GS, PPL = T::PPL;
   constexpr int NDOF = NDIM + 1, JG = NPE / PPL, NSIZE = NPE * NDOF;
+  constexpr bool FI = (FORM == FORM_FULLY_IMPLICIT);
+  constexpr double CS = FI ? 1.0 : T::CS;                       // continuity row sign
+  constexpr double CI = FI ? ((ET == CFDGPU_HEX8) ? 10.0 : 4.0) : T::CI;
+  constexpr bool SUPG = FI || T::SUPG;
   __shared__ ElemSmem<NDIM, NPE, NGP, JG> smem_all[GROUPS];
 
   const int grp = threadIdx.x / GS;
@@ -298,20 +311,30 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
     for (int a = 0; a < NDIM; a++) {
 #pragma unroll
       for (int c = 0; c < NDIM; c++) S.stress[gp][a][c] = mu * grad[a][c] - ((a == c) ? pres : 0.0);
-      double t1 = 0, t2 = 0, t3 = 0;
+      double r2;
+      if (FI) {
+        double g = 0;
 #pragma unroll
-      for (int c = 0; c < NDIM; c++) {
-        t1 += gP[a][c] * vel[c];
-        t2 += grad[a][c] * vP[c];
-        t3 += gP[a][c] * vP[c];
+        for (int c = 0; c < NDIM; c++) g += grad[a][c] * vel[c];
+        r2 = rho * (vD[a] + g - 0.0);
+      } else {
+        double t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+        for (int c = 0; c < NDIM; c++) {
+          t1 += gP[a][c] * vel[c];
+          t2 += grad[a][c] * vP[c];
+          t3 += gP[a][c] * vP[c];
+        }
+        r2 = rho * (vD[a] + (t1 + t2 - t3) - 0.0);
       }
-      const double r2 = rho * (vD[a] + (t1 + t2 - t3) - 0.0);
       S.res2[gp][a] = r2;
       S.rStab[gp][a] = r2 - mu * 0.0 + dp[a];
       tr += grad[a][a];
-      S.vP[gp][a] = vP[a];
+      // the tangent's advection velocity and gradient: the previous step's
+      // (semi-implicit) or the current iterate's (fully implicit)
+      S.vP[gp][a] = FI ? vel[a] : vP[a];
 #pragma unroll
-      for (int c = 0; c < NDIM; c++) S.gP[gp][a][c] = gP[a][c];
+      for (int c = 0; c < NDIM; c++) S.gP[gp][a][c] = FI ? grad[a][c] : gP[a][c];
     }
     S.trg[gp] = tr;
     // evaluateStabParams_algo3 with G = fact*I (2D: third diagonal entry 0)
@@ -319,8 +342,9 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
 #pragma unroll
     for (int a = 0; a < NDIM; a++) uGu += vP[a] * (fact * vP[a]);
     const double sumG2 = NDIM * (fact * fact);
-    double t0 = uGu + T::CI * (mu * mu / rho / rho) * sumG2;
+    double t0 = uGu + CI * (mu * mu / rho / rho) * sumG2;
     t0 = 1.0 / sqrt(t0);
+    S.tau2[gp] = P.stab2 / (t0 * (NDIM * fact));
     t0 = t0 / rho;
     S.tau0[gp] = t0 * P.stab0;
     S.tau1[gp] = t0 * P.stab1;
@@ -353,14 +377,14 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
       for (int a = 0; a < NDIM; a++) bb[a] = S.dN[gp][a][ii] * dvol;
       const double b4 = S.N[gp][ii] * dvol;
       const double b8 = af * b4;
-      const double tau0 = S.tau0[gp], tau1 = S.tau1[gp];
+      const double tau0 = S.tau0[gp], tau1 = S.tau1[gp], tau2 = S.tau2[gp];
       double vP[NDIM];
 #pragma unroll
       for (int a = 0; a < NDIM; a++) vP[a] = S.vP[gp][a];
       double Da = 0.0;
 #pragma unroll
       for (int a = 0; a < NDIM; a++) Da += vP[a] * bb[a];
-      Da = rho * Da * tau0;
+      Da = (FI && NDIM == 2) ? Da * tau0 : rho * Da * tau0;
 
       if (MODE != MODE_RESIDUAL || LIFT) {
         const CT cb8 = CT(b8), cDa = CT(Da), ctau1 = CT(tau1), caf = CT(af), cb4 = CT(b4);
@@ -402,10 +426,11 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
             acc[p][a][a] += f;
 #pragma unroll
             for (int c = 0; c < NDIM; c++) acc[p][a][c] += cb8 * gN[a][c];
-            acc[p][a][NDIM] -= cbb[a] * caf * Nj;
+            if (FI && NDIM == 3) acc[p][a][NDIM] -= cbb[a] * Nj;
+            else acc[p][a][NDIM] -= cbb[a] * caf * Nj;
           }
 #pragma unroll
-          for (int c = 0; c < NDIM; c++) acc[p][NDIM][c] += CT(T::CS) * (cb8 * dNj[c]);
+          for (int c = 0; c < NDIM; c++) acc[p][NDIM][c] += CT(CS) * (cb8 * dNj[c]);
           // Dj = af*gN + fact2*I | af*dN
           CT Dj[NDIM][NDOF];
 #pragma unroll
@@ -414,18 +439,36 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
             for (int c = 0; c < NDIM; c++) Dj[a][c] = gN[a][c] * caf + ((a == c) ? fact2 : CT(0));
             Dj[a][NDIM] = caf * dNj[a];
           }
-          if (T::SUPG) {
+          if (SUPG) {
 #pragma unroll
             for (int a = 0; a < NDIM; a++)
 #pragma unroll
               for (int c = 0; c < NDOF; c++) acc[p][a][c] += cDa * Dj[a][c];
+          }
+          if (FI) {
+            // derivative of the SUPG weight (u . grad N_i) tau0 [rho]
+            const CT c1 = (NDIM == 3) ? CT(tau0 * af * rho) * Nj : CT(tau0 * af) * Nj;
+#pragma unroll
+            for (int a = 0; a < NDIM; a++) {
+              const CT rs = CT(S.rStab[gp][a]);
+#pragma unroll
+              for (int c = 0; c < NDIM; c++) acc[p][a][c] += c1 * cbb[c] * rs;
+            }
           }
 #pragma unroll
           for (int c = 0; c < NDOF; c++) {
             CT s = CT(0);
 #pragma unroll
             for (int a = 0; a < NDIM; a++) s += cbb[a] * Dj[a][c];
-            acc[p][NDIM][c] += CT(T::CS) * (s * ctau1);
+            acc[p][NDIM][c] += CT(CS) * (s * ctau1);
+          }
+          if (FI && NDIM == 3) {
+            // LSIC
+            const CT f2 = CT(rho * af * tau2);
+#pragma unroll
+            for (int a = 0; a < NDIM; a++)
+#pragma unroll
+              for (int c = 0; c < NDIM; c++) acc[p][a][c] += (cbb[a] * dNj[c]) * f2;
           }
         }
       }
@@ -437,15 +480,20 @@ element_kernel(const int32_t *__restrict__ elems, int nel, const int32_t *__rest
           for (int c = 0; c < NDIM; c++) s += bb[c] * S.stress[gp][a][c];
           Fi[a] -= s;
         }
-        Fi[NDIM] -= T::CS * (b4 * S.trg[gp]);
-        if (T::SUPG) {
+        Fi[NDIM] -= CS * (b4 * S.trg[gp]);
+        if (SUPG) {
 #pragma unroll
           for (int a = 0; a < NDIM; a++) Fi[a] -= Da * S.rStab[gp][a];
         }
         double s = 0.0;
 #pragma unroll
         for (int a = 0; a < NDIM; a++) s += bb[a] * S.rStab[gp][a];
-        Fi[NDIM] -= T::CS * (tau1 * s);
+        Fi[NDIM] -= CS * (tau1 * s);
+        if (FI && NDIM == 3) {
+          const double f2 = tau2 * rho * S.trg[gp];
+#pragma unroll
+          for (int a = 0; a < NDIM; a++) Fi[a] -= bb[a] * f2;
+        }
       }
     }
   }

@@ -160,6 +160,14 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
   if (options.count("-gpu_inner_rtol")) opts_.inner_rtol = std::atof(options["-gpu_inner_rtol"].c_str());
   if (options.count("-gpu_refine_rtol")) opts_.refine_rtol = std::atof(options["-gpu_refine_rtol"].c_str());
   if (options.count("-gpu_newton_rtol")) opts_.newton_rtol = std::atof(options["-gpu_newton_rtol"].c_str());
+  {
+    const std::string f = get("-gpu_formulation", "semi_implicit");
+    if (f == "fully_implicit") opts_.formulation = CFDGPU_FORM_FULLY_IMPLICIT;
+    else if (f != "semi_implicit") {
+      std::cerr << " -gpu_formulation must be semi_implicit or fully_implicit" << std::endl;
+      return CFDGPU_EINVAL;
+    }
+  }
 
   std::vector<double> xyz((size_t)nNode_global * ndim), dv(nDBC);
   std::vector<int32_t> conn((size_t)nElem_global * npElem), dn(nDBC), dd(nDBC);

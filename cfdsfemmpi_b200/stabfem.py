@@ -13,6 +13,8 @@ plus this library's own keys:
 
   -gpu_precision fp64|mixed   -gpu_inner_restart m    -gpu_inner_rtol r
   -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_newton_rtol r
+  -gpu_formulation semi_implicit|fully_implicit   (element routine; the
+        reference's active one, or its commented-out fully-implicit one)
   -gpu_guess constant|extrapolation   (Newton initial guess; constant = the
                                        reference's, extrapolation = u_n plus
                                        the min-residual multiple of u_n - u_{n-1})
@@ -78,6 +80,8 @@ def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
         kw["newton_rtol"] = float(opts["-gpu_newton_rtol"])
     if "-gpu_guess" in opts:
         kw["guess"] = opts["-gpu_guess"].lower()
+    if "-gpu_formulation" in opts:
+        kw["formulation"] = opts["-gpu_formulation"].lower()
     kw["_notes"] = notes
     return kw
 
@@ -147,6 +151,8 @@ class StabFEM:
         s = f"GMRES({k['restart']}) pc={k['pc']} rtol={k['rtol']:g} max_it={k['max_it']} precision={k['precision']}"
         if k.get("guess", "constant") != "constant":
             s += f" guess={k['guess']}"
+        if k.get("formulation", "semi_implicit") != "semi_implicit":
+            s += f" formulation={k['formulation']}"
         if k.get("_notes"):
             s += " [" + "; ".join(k["_notes"]) + "]"
         return s

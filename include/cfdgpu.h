@@ -96,7 +96,13 @@ typedef struct cfdgpu_solver_opts {
   int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
   double refine_rtol;       /* mixed mode: refinement target ||b - A32 x|| <= max(refine_rtol ||b||, newton_tol/10) (0: 1e-10) */
   double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0|| (0: off, the reference's test only) */
+  int formulation;          /* CFDGPU_FORM_*: element routine (0: the reference's active semi-implicit one) */
 } cfdgpu_solver_opts;
+
+/* element formulations */
+#define CFDGPU_FORM_SEMI_IMPLICIT 0   /* active "semi-implicit type B" routines; tangent reusable in a step */
+#define CFDGPU_FORM_FULLY_IMPLICIT 1  /* the reference's commented-out fully-implicit routines (SUPG+PSPG, LSIC in
+                                         3D, full Newton tangent); reuse_tangent is ignored */
 
 #define CFDGPU_MAX_NEWTON 32
 

@@ -360,6 +360,198 @@ int orc_element(int et, const double *X, const double *prev, const double *cur,
   return neg ? -1 : 0;
 }
 
+/*
+ * Fully-implicit element routine: the reference's commented-out variant
+ * "Fully-implicit formulation" (quad4 LagrangeElem2DNavierStokesQuad4Node.cpp:117-396,
+ * tri3 LagrangeElem2DNavierStokesTria3Node.cpp:117-396, hex8
+ * LagrangeElem3DNavierStokesHexa8Node.cpp:109-432, tet4
+ * LagrangeElem3DNavierStokesTetra4Node.cpp:115-438).  Convection is
+ * grad(u_cur) u_cur with its full Newton linearisation, SUPG and PSPG act on
+ * the current velocity, LSIC is active in 3D (scaled by elemData[10]), and no
+ * row is sign-flipped.  The 2D and 3D texts differ and are kept as written:
+ * 2D SUPG has no rho factor and its pressure column carries af; 3D SUPG has
+ * rho, its pressure column has no af; CI is 10 for hex8 and 4 otherwise.
+ * Same arguments and return value as orc_element.
+ */
+int orc_element_fi(int et, const double *X, const double *prev, const double *cur,
+                   const double *dotcur, const double *elemData, const double *td,
+                   double *K, double *F, double *info)
+{
+  int ndim, npe, ngp;
+  einfo(et, &ndim, &npe, &ngp);
+  const int ndof = ndim + 1, nsize = npe * ndof;
+  double gpx[8][3], gw[8];
+  gauss_points(et, gpx, gw);
+
+  double Nv[8][8], Dx[8][8], Dy[8][8], Dz[8][8], dv[8];
+  double elemVol = 0.0;
+  int neg = 0;
+  for (int gp = 0; gp < ngp; gp++) {
+    double Jac;
+    basis_phys(et, ndim, npe, gpx[gp], X, Nv[gp], Dx[gp], Dy[gp], Dz[gp], &Jac);
+    if (Jac < 0.0) neg = 1;
+    dv[gp] = gw[gp] * Jac;
+    elemVol += dv[gp];
+  }
+  double charlen = (ndim == 2) ? sqrt(4.0 * fabs(elemVol) / ORC_PI)
+                               : pow(6.0 * fabs(elemVol) / ORC_PI, 1.0 / 3.0);
+  if (info) { info[0] = elemVol; info[1] = charlen; }
+
+  const double CI = (et == ORC_HEX8) ? 10.0 : 4.0;
+  double fact = 4.0 / charlen / charlen;
+  double G[3] = {fact, fact, (ndim == 3) ? fact : 0.0};
+  double sumG2 = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+  double trG = G[0] + G[1] + G[2];
+
+  const double rho = elemData[0], mu = elemData[1];
+  const double af = td[2], acceFact = td[8];
+  const double muTaf = mu * af;
+
+  memset(K, 0, sizeof(double) * nsize * nsize);
+  memset(F, 0, sizeof(double) * nsize);
+
+  for (int gp = 0; gp < ngp; gp++) {
+    const double *N = Nv[gp];
+    const double *dN[3] = {Dx[gp], Dy[gp], Dz[gp]};
+    double velPrev[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, velDot[3] = {0, 0, 0}, dp[3] = {0, 0, 0};
+    double grad[3][3] = {{0}};
+    double pres = 0.0;
+    for (int ii = 0; ii < npe; ii++) {
+      const int TI = ii * ndof;
+      for (int a = 0; a < ndim; a++) velPrev[a] += prev[TI + a] * N[ii];
+      for (int a = 0; a < ndim; a++) {
+        double b = cur[TI + a];
+        vel[a] += b * N[ii];
+        for (int c = 0; c < ndim; c++) grad[a][c] += b * dN[c][ii];
+      }
+      double b4 = cur[TI + ndim];
+      pres += b4 * N[ii];
+      for (int c = 0; c < ndim; c++) dp[c] += b4 * dN[c][ii];
+      for (int a = 0; a < ndim; a++) velDot[a] += dotcur[TI + a] * N[ii];
+    }
+    double stress[3][3];
+    for (int a = 0; a < ndim; a++)
+      for (int c = 0; c < ndim; c++) stress[a][c] = mu * grad[a][c];
+    for (int a = 0; a < ndim; a++) stress[a][a] -= pres;
+    double res2[3], rStab[3], tr = 0.0;
+    for (int a = 0; a < ndim; a++) {
+      double g = 0.0;
+      for (int c = 0; c < ndim; c++) g += grad[a][c] * vel[c];
+      res2[a] = rho * (velDot[a] + g - 0.0);
+      rStab[a] = res2[a] - mu * 0.0 + dp[a];
+      tr += grad[a][a];
+    }
+    /* evaluateStabParams_algo3 at velPrev */
+    double uGu = 0.0;
+    for (int a = 0; a < 3; a++) {
+      double ua = (a < ndim) ? velPrev[a] : 0.0;
+      uGu += ua * (G[a] * ua);
+    }
+    double tau0 = uGu + CI * (mu * mu / rho / rho) * sumG2;
+    tau0 = 1.0 / sqrt(tau0);
+    double tau2 = 1.0 / (tau0 * trG);
+    tau0 = tau0 / rho;
+    double tau1 = tau0;
+    tau0 *= elemData[8];
+    tau1 *= elemData[9];
+    tau2 *= elemData[10];
+
+    const double dvol = dv[gp];
+    for (int ii = 0; ii < npe; ii++) {
+      const int TI = ndof * ii;
+      double bb[3], b4, bm[3], b8;
+      for (int a = 0; a < ndim; a++) bb[a] = dN[a][ii] * dvol;
+      b4 = N[ii] * dvol;
+      for (int a = 0; a < ndim; a++) bm[a] = muTaf * bb[a];
+      b8 = af * b4;
+      double Da = 0.0;
+      for (int a = 0; a < ndim; a++) Da += vel[a] * bb[a];
+      Da = (ndim == 3) ? Da * tau0 * rho : Da * tau0;
+
+      for (int jj = 0; jj < npe; jj++) {
+        const int TJ = ndof * jj;
+        double fact2 = rho * acceFact * N[jj];
+        double f = b4 * fact2;
+        double dif = 0.0;
+        for (int a = 0; a < ndim; a++) dif += bm[a] * dN[a][jj];
+        f += dif;
+        for (int a = 0; a < ndim; a++) K[(TI + a) * nsize + TJ + a] += f;
+
+        double gradN[3][3];
+        for (int a = 0; a < ndim; a++)
+          for (int c = 0; c < ndim; c++) gradN[a][c] = grad[a][c] * (rho * N[jj]);
+        double Db = 0.0;
+        for (int a = 0; a < ndim; a++) Db += vel[a] * dN[a][jj];
+        Db = rho * Db;
+        for (int a = 0; a < ndim; a++) gradN[a][a] += Db;
+        if (ndim == 3) {
+          for (int a = 0; a < ndim; a++)
+            for (int c = 0; c < ndim; c++) gradN[a][c] *= af;
+          for (int a = 0; a < ndim; a++)
+            for (int c = 0; c < ndim; c++) K[(TI + a) * nsize + TJ + c] += (b4 * gradN[a][c]);
+          for (int a = 0; a < ndim; a++) K[(TI + a) * nsize + TJ + ndim] -= (bb[a] * N[jj]);
+        } else {
+          for (int a = 0; a < ndim; a++)
+            for (int c = 0; c < ndim; c++) K[(TI + a) * nsize + TJ + c] += (b8 * gradN[a][c]);
+          for (int a = 0; a < ndim; a++) K[(TI + a) * nsize + TJ + ndim] -= (bb[a] * af * N[jj]);
+        }
+        for (int c = 0; c < ndim; c++) K[(TI + ndim) * nsize + TJ + c] += (b8 * dN[c][jj]);
+        if (ndim == 2)
+          for (int a = 0; a < ndim; a++)
+            for (int c = 0; c < ndim; c++) gradN[a][c] *= af;
+
+        double Dj[3][4];
+        for (int a = 0; a < ndim; a++) {
+          for (int c = 0; c < ndim; c++) Dj[a][c] = gradN[a][c] + ((a == c) ? fact2 : 0.0);
+          Dj[a][ndim] = af * dN[a][jj];
+        }
+        /* SUPG */
+        for (int a = 0; a < ndim; a++)
+          for (int c = 0; c <= ndim; c++) K[(TI + a) * nsize + TJ + c] += Da * Dj[a][c];
+        const double c1 = (ndim == 3) ? tau0 * af * rho * N[jj] : (tau0 * af);
+        for (int a = 0; a < ndim; a++)
+          for (int c = 0; c < ndim; c++) {
+            if (ndim == 3) K[(TI + a) * nsize + TJ + c] += (c1 * bb[c] * rStab[a]);
+            else K[(TI + a) * nsize + TJ + c] += (c1 * bb[c] * rStab[a] * N[jj]);
+          }
+        /* PSPG */
+        for (int c = 0; c <= ndim; c++) {
+          double s = 0.0;
+          for (int a = 0; a < ndim; a++) s += bb[a] * Dj[a][c];
+          K[(TI + ndim) * nsize + TJ + c] += s * tau1;
+        }
+        /* LSIC (3D only; commented out in the 2D text) */
+        if (ndim == 3) {
+          double f2 = rho * af * tau2;
+          for (int a = 0; a < ndim; a++)
+            for (int c = 0; c < ndim; c++) K[(TI + a) * nsize + TJ + c] += (bb[a] * dN[c][jj]) * f2;
+        }
+      }
+
+      for (int a = 0; a < ndim; a++) {
+        double s = b4 * res2[a];
+        for (int c = 0; c < ndim; c++) s += bb[c] * stress[a][c];
+        F[TI + a] -= s;
+      }
+      F[TI + ndim] -= (b4 * tr);
+      for (int a = 0; a < ndim; a++) F[TI + a] -= Da * rStab[a];
+      double s = 0.0;
+      for (int a = 0; a < ndim; a++) s += bb[a] * rStab[a];
+      F[TI + ndim] -= (tau1 * s);
+      if (ndim == 3) {
+        double f2 = tau2 * rho * tr;
+        for (int a = 0; a < ndim; a++) F[TI + a] -= bb[a] * f2;
+      }
+    }
+  }
+  return neg ? -1 : 0;
+}
+
+/* element formulation used by orc_assemble: 0 = semi-implicit type B (the
+ * reference's active routine), 1 = fully implicit (orc_element_fi) */
+static int g_form = 0;
+void orc_set_formulation(int form) { g_form = form; }
+
 /* ---------------- free-dof pattern (StabFEM2.cpp:57-81, 192-227) -------- */
 
 /* node -> sorted unique neighbour nodes (nodes sharing an element) */
@@ -474,7 +666,8 @@ static int assemble_one(int et, int e, int ndim, int npe, const int *conn, const
       gdof[a * ndof + d] = (int)g;
     }
   }
-  int rc = orc_element(et, X, pv, cv, dc, elemData, td, K, F, NULL);
+  int rc = g_form ? orc_element_fi(et, X, pv, cv, dc, elemData, td, K, F, NULL)
+                  : orc_element(et, X, pv, cv, dc, elemData, td, K, F, NULL);
   if (iter == 0) {                                  /* StabFEM2.cpp:678-703 */
     for (int ii = 0; ii < nsize; ii++) {
       if (fa[ii] == -1) {

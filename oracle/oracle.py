@@ -50,6 +50,10 @@ def lib():
         L.orc_element.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                   ctypes.c_void_p]
         L.orc_element.restype = ctypes.c_int
+        L.orc_element_fi.argtypes = L.orc_element.argtypes
+        L.orc_element_fi.restype = ctypes.c_int
+        L.orc_set_formulation.argtypes = [ctypes.c_int]
+        L.orc_set_formulation.restype = None
         L.orc_pattern.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p, _i32p,
                                   ctypes.c_int, _i32p, ctypes.c_void_p]
         L.orc_pattern.restype = ctypes.c_long
@@ -77,15 +81,21 @@ def lib():
 ELEM_INFO = {0: (2, 3, 1), 1: (2, 4, 4), 2: (3, 4, 1), 3: (3, 8, 8)}  # ndim, npe, ngp
 
 
-def element(et: int, X, prev, cur, dotcur, elem_data, td):
-    """K (nsize x nsize) and F of one element; also (elemVol, charlen)."""
+FORMULATIONS = {"semi_implicit": 0, "fully_implicit": 1}
+
+
+def element(et: int, X, prev, cur, dotcur, elem_data, td, form: str = "semi_implicit"):
+    """K (nsize x nsize) and F of one element; also (elemVol, charlen).
+    form: "semi_implicit" (the reference's active type-B routine) or
+    "fully_implicit" (its commented-out fully-implicit routine)."""
     ndim, npe, _ = ELEM_INFO[et]
     ndof = ndim + 1
     nsize = npe * ndof
     K = np.zeros(nsize * nsize)
     F = np.zeros(nsize)
     info = np.zeros(2)
-    rc = lib().orc_element(et, np.ascontiguousarray(X, dtype=np.float64).ravel(),
+    fn = lib().orc_element_fi if FORMULATIONS[form] else lib().orc_element
+    rc = fn(et, np.ascontiguousarray(X, dtype=np.float64).ravel(),
                            np.ascontiguousarray(prev, dtype=np.float64).ravel(),
                            np.ascontiguousarray(cur, dtype=np.float64).ravel(),
                            np.ascontiguousarray(dotcur, dtype=np.float64).ravel(),
@@ -133,8 +143,10 @@ class OracleFEM:
 
     def __init__(self, mesh, ctrl, solver: str = "gmres", restart: int = 50, rtol: float = 1e-10,
                  atol: float = 1e-50, dtol: float = 1e4, max_it: int = 10000, pc: str = "jacobi",
-                 threads: int = 1, newton_tol: float = 1e-8, newton_max: int = 10, verbose: bool = False):
+                 threads: int = 1, newton_tol: float = 1e-8, newton_max: int = 10, verbose: bool = False,
+                 form: str = "semi_implicit"):
         self.mesh = mesh
+        self.form = FORMULATIONS[form]
         self.ctrl = ctrl
         self.solver = solver
         self.restart, self.rtol, self.atol, self.dtol, self.max_it = restart, rtol, atol, dtol, max_it
@@ -212,6 +224,7 @@ class OracleFEM:
         self.solnDotCur = td[1] * self.solnDot + (1.0 - td[1]) * self.solnDotPrev
 
     def assemble(self, it: int, want_K: bool = True) -> int:
+        lib().orc_set_formulation(self.form)
         return lib().orc_assemble(self.et, self.mesh.nNode, self.mesh.nElem, self.conn, self.coords, self.dofmap,
                                   self.solnPrev, self.solnCur, self.solnDotCur, self.solnApplied, self.elem_data,
                                   self.td, it, 1 if want_K else 0, self.rowptr, self.colidx, self.nnz, self.vals,

@@ -72,13 +72,16 @@ def test_gmres_matches_lu_2d():
     assert 50 < min(its) and max(its) < 200
 
 
+@pytest.mark.parametrize("form", ["semi_implicit", "fully_implicit"])
 @pytest.mark.parametrize("et", [0, 1, 2, 3])
-def test_tangent_matches_finite_difference(et):
+def test_tangent_matches_finite_difference(et, form):
     """diffStiffTest analogue (src/base/StabFEM.cpp:581-706): K = -dF/dsoln.
 
     solnCur = af*soln + (1-af)*solnPrev and solnDotCur = am*(td9*soln + ...)
     so dF/dsoln = af dF/dcur + am td9 dF/ddotcur; the element's acceFact td[8]
     equals am*td9 for gen-alpha, so K must match the chain-rule derivative.
+    The fully-implicit routine is nonlinear in soln (convection, SUPG weight)
+    and its K is the full Newton tangent, LSIC included (active here).
     """
     rng = np.random.default_rng(7 + et)
     ndim, npe, _ = oracle.ELEM_INFO[et]
@@ -88,7 +91,8 @@ def test_tangent_matches_finite_difference(et):
            3: [[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]]}[et]
     X = 0.1 * np.array(ref, dtype=float) + 0.01 * rng.standard_normal((npe, ndim))
     td = oracle.time_params(2, 0.0, 0.1)
-    ed = np.zeros(50); ed[0] = 1.0; ed[1] = 0.01; ed[8:11] = (1.0, 1.0, 0.0)
+    ed = np.zeros(50); ed[0] = 1.0; ed[1] = 0.01
+    ed[8:11] = (1.0, 1.0, 0.0) if form == "semi_implicit" else (1.0, 1.0, 1.0)
     prev = rng.standard_normal((npe, ndof)) * 0.3
     dotprev = rng.standard_normal((npe, ndof)) * 0.1
     soln = rng.standard_normal((npe, ndof)) * 0.3
@@ -97,7 +101,7 @@ def test_tangent_matches_finite_difference(et):
         cur = td[2] * s + (1 - td[2]) * prev
         dot = td[9] * s + td[10] * prev + td[15] * dotprev
         dotcur = td[1] * dot + (1 - td[1]) * dotprev
-        K, F, info, rc = oracle.element(et, X, prev, cur, dotcur, ed, td)
+        K, F, info, rc = oracle.element(et, X, prev, cur, dotcur, ed, td, form=form)
         return K, F
 
     K, _ = F_of(soln)
