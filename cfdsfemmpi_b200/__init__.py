@@ -7,7 +7,7 @@ path; this package is the host side: the reference's file formats (io), the
 generators (meshgen) and a VTU writer (vtu).
 """
 from . import io, meshgen
-from ._lib import CfdGpuError, Handle, load, pattern_build
+from ._lib import Batch, CfdGpuError, Handle, load, pattern_build
 from .stabfem import StabFEM, solver_options_from_petsc
 
 __all__ = ["io", "meshgen", "Handle", "CfdGpuError", "load", "pattern_build", "StabFEM", "solver_options_from_petsc"]

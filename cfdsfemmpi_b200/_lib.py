@@ -24,6 +24,8 @@ EXPORTS = [
     "cfdgpu_mpnn_create", "cfdgpu_mpnn_destroy", "cfdgpu_mpnn_num_params", "cfdgpu_mpnn_get_params",
     "cfdgpu_mpnn_set_params", "cfdgpu_mpnn_set_scales", "cfdgpu_mpnn_add_sample", "cfdgpu_mpnn_num_samples",
     "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess_mode", "cfdgpu_set_guess",
+    "cfdgpu_batch_create", "cfdgpu_batch_destroy", "cfdgpu_batch_last_error", "cfdgpu_batch_size",
+    "cfdgpu_batch_handle", "cfdgpu_batch_set_schedule", "cfdgpu_batch_get_schedule", "cfdgpu_batch_step",
 ]
 GUESS = {"network": 1, "network_velocity": 2, "extrapolation": 4}
 FORM = {"semi_implicit": 0, "fully_implicit": 1}
@@ -129,13 +131,25 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_mpnn_predict.argtypes = [vp, vp, vp, vp]
     L.cfdgpu_set_guess.argtypes = [vp, vp]
     L.cfdgpu_set_guess_mode.argtypes = [vp, vp, ip]
+    L.cfdgpu_batch_create.argtypes = [ip, ctypes.POINTER(Mesh), ctypes.POINTER(Control), ctypes.POINTER(SolverOpts),
+                                      ctypes.POINTER(vp)]
+    L.cfdgpu_batch_destroy.argtypes = [vp]
+    L.cfdgpu_batch_last_error.argtypes = [vp]
+    L.cfdgpu_batch_last_error.restype = ctypes.c_char_p
+    L.cfdgpu_batch_size.argtypes = [vp]
+    L.cfdgpu_batch_handle.argtypes = [vp, ip]
+    L.cfdgpu_batch_handle.restype = vp
+    L.cfdgpu_batch_set_schedule.argtypes = [vp, ip, ip]
+    L.cfdgpu_batch_get_schedule.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]
+    L.cfdgpu_batch_step.argtypes = [vp, vp, vp, ctypes.POINTER(StepStats), vp]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
     L.cfdgpu_set_profiling.argtypes = [vp, ip]
     L.cfdgpu_kernel_stats.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:
-        if name not in ("cfdgpu_last_error", "cfdgpu_launch_count"):
+        if name not in ("cfdgpu_last_error", "cfdgpu_launch_count", "cfdgpu_batch_last_error", "cfdgpu_batch_handle"):
             getattr(L, name).restype = ctypes.c_int
     _LIB = L
     return L
@@ -165,6 +179,17 @@ def _mesh_struct(mesh):
     m = Mesh(mesh.ndim, mesh.npElem, mesh.nNode, mesh.nElem, _ptr(coords), _ptr(conn), mesh.nDBC, _ptr(dn), _ptr(dd),
              _ptr(dv))
     return m, (coords, conn, dn, dd, dv)
+
+
+def _control_opts(ctrl, restart=50, rtol=1e-10, atol=1e-50, dtol=1e4, max_it=10000, pc="jacobi", precision="fp64",
+                  inner_restart=0, inner_rtol=1e-4, reuse_tangent=True, newton_tol=1e-8, newton_max_iter=10,
+                  refine_rtol=1e-10, newton_rtol=0.0, formulation="semi_implicit"):
+    """(Control, SolverOpts) structs from an io.Control and solver keywords."""
+    c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
+                ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
+    o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
+                   1 if reuse_tangent else 0, refine_rtol, newton_rtol, FORM[formulation])
+    return c, o
 
 
 def pattern_build(mesh) -> dict:
@@ -202,14 +227,13 @@ class Handle:
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()
-        self.ndim, self.npe = mesh.ndim, mesh.npElem
-        self.ndof = mesh.ndim + 1
-        self.nNode, self.nElem = mesh.nNode, mesh.nElem
+        self._owned = True
+        self._set_sizes(mesh)
         m, self._keep = _mesh_struct(mesh)
-        c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
-                    ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
-        o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
-                       1 if reuse_tangent else 0, refine_rtol, newton_rtol, FORM[formulation])
+        c, o = _control_opts(ctrl, restart=restart, rtol=rtol, atol=atol, dtol=dtol, max_it=max_it, pc=pc,
+                             precision=precision, inner_restart=inner_restart, inner_rtol=inner_rtol,
+                             reuse_tangent=reuse_tangent, newton_tol=newton_tol, newton_max_iter=newton_max_iter,
+                             refine_rtol=refine_rtol, newton_rtol=newton_rtol, formulation=formulation)
         rc = L.cfdgpu_create(ctypes.byref(m), ctypes.byref(c), ctypes.byref(o), ctypes.byref(self.h))
         if rc != 0:
             msg = L.cfdgpu_last_error(self.h).decode() if self.h else "create failed"
@@ -221,14 +245,30 @@ class Handle:
         elif guess != "constant":
             raise ValueError(f"guess must be 'constant' or 'extrapolation', not {guess!r}")
 
+    def _set_sizes(self, mesh):
+        self.ndim, self.npe = mesh.ndim, mesh.npElem
+        self.ndof = mesh.ndim + 1
+        self.nNode, self.nElem = mesh.nNode, mesh.nElem
+
+    @classmethod
+    def _borrow(cls, hptr, mesh, owner):
+        """Non-owning view of a handle that another object (a Batch) owns."""
+        self = cls.__new__(cls)
+        self._L = load()
+        self.h = ctypes.c_void_p(hptr)
+        self._owned = False
+        self._owner = owner
+        self._set_sizes(mesh)
+        return self
+
     def _check(self, rc: int):
         if rc != 0:
             raise CfdGpuError(rc, self._L.cfdgpu_last_error(self.h).decode())
 
     def close(self):
-        if self.h:
+        if self.h and self._owned:
             self._L.cfdgpu_destroy(self.h)
-            self.h = ctypes.c_void_p()
+        self.h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -443,3 +483,74 @@ class Mpnn:
 
     def detach(self):
         self._check(self._L.cfdgpu_set_guess(self.handle.h, None))
+
+
+class Batch:
+    """Owning wrapper of a cfdgpu_batch: many independent instances (each an
+    (io.Mesh, io.Control) pair with the same solver keywords) stepped
+    concurrently on the current device."""
+
+    def __init__(self, cases, **solver_kw):
+        L = load()
+        self._L = L
+        self.b = ctypes.c_void_p()
+        self.cases = list(cases)
+        n = len(self.cases)
+        ms = (Mesh * n)()
+        cs = (Control * n)()
+        os_ = (SolverOpts * n)()
+        self._keep = []
+        for i, (mesh, ctrl) in enumerate(self.cases):
+            m, keep = _mesh_struct(mesh)
+            c, o = _control_opts(ctrl, **solver_kw)
+            ms[i], cs[i], os_[i] = m, c, o
+            self._keep.append(keep)
+        rc = L.cfdgpu_batch_create(n, ms, cs, os_, ctypes.byref(self.b))
+        if rc != 0:
+            msg = L.cfdgpu_batch_last_error(self.b).decode() if self.b else "batch create failed"
+            if self.b:
+                L.cfdgpu_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+            raise CfdGpuError(rc, msg)
+        self.handles = [Handle._borrow(L.cfdgpu_batch_handle(self.b, i), mesh, self)
+                        for i, (mesh, _) in enumerate(self.cases)]
+
+    def __len__(self):
+        return len(self.cases)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CfdGpuError(rc, self._L.cfdgpu_batch_last_error(self.b).decode())
+
+    def set_schedule(self, concurrency: int = 0, chunk: int = 0):
+        """(0, 0): autotune over the next batch steps."""
+        self._check(self._L.cfdgpu_batch_set_schedule(self.b, concurrency, chunk))
+
+    def schedule(self):
+        c, ch, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.cfdgpu_batch_get_schedule(self.b, ctypes.byref(c), ctypes.byref(ch), ctypes.byref(t)))
+        return {"concurrency": c.value, "chunk": ch.value, "tuned": bool(t.value)}
+
+    def step(self, times):
+        """One step of every instance at times[i] (ramp factor min(t, 1)).
+        Returns (list of StepStats, per-instance host latency in ms)."""
+        n = len(self.cases)
+        tn = np.ascontiguousarray(times, dtype=np.float64)
+        tf = np.minimum(tn, 1.0)
+        st = (StepStats * n)()
+        lat = np.zeros(n)
+        self._check(self._L.cfdgpu_batch_step(self.b, _ptr(tn), _ptr(tf), st, _ptr(lat)))
+        return list(st), lat
+
+    def close(self):
+        if self.b:
+            for h in self.handles:
+                h.h = ctypes.c_void_p()
+            self._L.cfdgpu_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -85,7 +85,9 @@ struct cfdgpu_handle {
   double *h_scalar = nullptr;        // pinned host mirror
   GmresState *h_gst = nullptr;       // pinned
   bool assembled_K = false;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
+  bool blocking = false;   // host waits sleep (cudaEventBlockingSync) instead of spinning
+  int chunk = 8;           // Arnoldi steps enqueued (and replayed as one graph) between host polls
   // learned initial guess
   cfdgpu_mpnn *guess = nullptr;
   int guess_mode = 0;
@@ -498,12 +500,26 @@ static int norm2_dev(cfdgpu_handle *h, const double *x, double *d_out)
   return check_launch(h, "norm2");
 }
 
+// Wait on the host for everything enqueued on the handle's stream.  A handle
+// driven by one of many host threads (cfdgpu_batch_*) sleeps in the wait
+// instead of spinning, so that dozens of such threads can share a few cores.
+static int host_wait(cfdgpu_handle *h)
+{
+  if (!h->blocking) {
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+  }
+  CK(cudaEventRecord(h->evw, h->stream));
+  CK(cudaEventSynchronize(h->evw));
+  return 0;
+}
+
 static int norm2(cfdgpu_handle *h, const double *x, double *out_host)
 {
   int rc = norm2_dev(h, x, h->scalar);
   if (rc) return rc;
   CK(cudaMemcpyAsync(h->h_scalar, h->scalar, sizeof(double) * 1, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  if ((rc = host_wait(h))) return rc;
   *out_host = h->h_scalar[0];
   return 0;
 }
@@ -544,7 +560,7 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
   const int vgrid = grid_for(n);
   // Arnoldi steps j0..j0+CH-1 enqueued as one unit: directly, or (without
   // per-kernel profiling) as a CUDA graph captured once per chunk and reused
-  const int CH = 8;
+  const int CH = h->chunk;
   auto enqueue_chunk = [&](int j0) -> int {
     for (int j = j0; j < std::min(m, j0 + CH); j++) {
       int r;
@@ -605,7 +621,7 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
     h->launches += 1;
     if ((rc = check_launch(h, "gmres_build_soln"))) return rc;
     CK(cudaMemcpyAsync(h->h_gst, st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    if ((rc = host_wait(h))) return rc;
     GmresState s = h->h_gst[0];
     int reason = s.reason;
     if (reason == 0 && s.its >= max_it) reason = -3;   // KSP_DIVERGED_ITS
@@ -720,13 +736,47 @@ static int check_negjac(cfdgpu_handle *h)
 {
   int v = 0;
   CK(cudaMemcpyAsync(&v, h->negjac, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  if (int rc = host_wait(h)) return rc;
   if (v) {
     h->err = "Negative Jacobian in the element routine";
     return CFDGPU_ENEGJAC;
   }
   return 0;
 }
+
+namespace cfdgpu {
+
+int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk)
+{
+  if (!h || chunk < 1 || chunk > 64) return CFDGPU_EINVAL;
+  if (blocking != h->blocking) {
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    const unsigned flags = cudaEventDisableTiming | (blocking ? cudaEventBlockingSync : 0u);
+    for (auto &x : e) CK(cudaEventCreateWithFlags(&x, flags));
+    CK(cudaStreamSynchronize(h->stream));
+    cudaEventDestroy(h->ev0); cudaEventDestroy(h->ev1); cudaEventDestroy(h->evw);
+    h->ev0 = e[0]; h->ev1 = e[1]; h->evw = e[2];
+    h->blocking = blocking;
+  }
+  if (chunk != h->chunk) {
+    // the cached Arnoldi graphs hold chunk-length pieces of the cycle
+    CK(cudaStreamSynchronize(h->stream));
+    for (auto &g : h->graphs64) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &g : h->graphs32) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    h->chunk = chunk;
+  }
+  return 0;
+}
+
+int handle_work(cfdgpu_handle *h, double *dofs, double *blocks)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (dofs) *dofs = (double)h->n;
+  if (blocks) *blocks = (double)h->topo.nnzb();
+  return 0;
+}
+
+}  // namespace cfdgpu
 
 namespace cfdgpu {
 int handle_graph(cfdgpu_handle *h, GraphView *out)
@@ -780,6 +830,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&h->ev0, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev1, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->evw, cudaEventDisableTiming));
   int rc = 0;
   const int64_t n = h->n;
   std::vector<int32_t> diag(h->nNode);
@@ -883,6 +934,7 @@ int cfdgpu_destroy(cfdgpu_handle *h)
   for (auto g : h->graphs32) if (g) cudaGraphExecDestroy(g);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->evw) cudaEventDestroy(h->evw);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return 0;
@@ -964,7 +1016,7 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
                                                              h->red_partial2, h->red_counter, h->scalar + 2);
       LAUNCHED(h);
       CK(cudaMemcpyAsync(h->h_scalar + 2, h->scalar + 2, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-      CK(cudaStreamSynchronize(h->stream));
+      if ((rc = host_wait(h))) return rc;
       const double r1 = h->h_scalar[2], r2 = h->h_scalar[3], g11 = h->h_scalar[4], g12 = h->h_scalar[5],
                    g22 = h->h_scalar[6];
       double a1 = 0.0, a2 = 0.0;
@@ -1053,10 +1105,10 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     k_axpy<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, 1.0, h->dx, h->soln);
     LAUNCHED(h);
     if ((rc = check_launch(h, "axpy"))) return rc;
-    CK(cudaStreamSynchronize(h->stream));
+    if ((rc = host_wait(h))) return rc;
     ms_sol += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
   }
-  CK(cudaStreamSynchronize(h->stream));
+  if ((rc = host_wait(h))) return rc;
   stats->ms_assembly = ms_asm;
   stats->ms_solver = ms_sol;
   stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tstart).count();

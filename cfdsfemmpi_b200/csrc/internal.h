@@ -20,6 +20,14 @@ struct GraphView {
 // device view of a handle's mesh graph
 int handle_graph(cfdgpu_handle *h, GraphView *out);
 
+// host-side scheduling of a handle's step: blocking (sleeping) host waits and
+// the number of Arnoldi steps per graph chunk (1..64); results do not depend
+// on either (Arnoldi kernels after convergence are no-ops)
+int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk);
+
+// size of a handle's system: dofs and BSR blocks (work estimate)
+int handle_work(cfdgpu_handle *h, double *dofs, double *blocks);
+
 // guess model attached to a handle: given u_n (solnPrev after the time
 // update) and u_{n-1} (solnPrev2), write the predicted increment for every
 // dof into delta (device, nNode*ndof); returns 0 on success

@@ -101,6 +101,18 @@ def case_hex(n: int, steps: int, mu: float = 0.001, dt: float = 0.1):
     return cavity3d(n), control_for(steps, dt, mu), dict(GMRES_OPTIONS)
 
 
+def batch_cases(count: int = 64, n_lo: int = 24, n_hi: int = 160, re_lo: float = 100.0, re_hi: float = 5000.0,
+                dt: float = 0.05, steps: int = 100, seed: int = 2024):
+    """Independent 2D lid-driven cavities of uneven size and Reynolds number:
+    n ~ U{n_lo..n_hi} elements per side, log Re ~ U[log re_lo, log re_hi]
+    (unit lid speed and side, rho 1, so mu = 1/Re), all from rest.
+    Returns [(mesh, control, n, Re)]."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_lo, n_hi + 1, count)
+    res = np.exp(rng.uniform(np.log(re_lo), np.log(re_hi), count))
+    return [(cavity2d(int(n)), control_for(steps, dt, 1.0 / float(re)), int(n), float(re)) for n, re in zip(ns, res)]
+
+
 def write_case(directory: str, name: str, mesh: Mesh, ctrl: Control, opts: dict) -> Tuple[str, str, str]:
     """Write mesh/control/options files; returns (mesh prefix, control path, options path)."""
     os.makedirs(directory, exist_ok=True)

@@ -285,6 +285,38 @@ int cfdgpu_set_profiling(cfdgpu_handle *h, int on);
  * summed algorithmic bytes (the minimum DRAM traffic of each launch). */
 int cfdgpu_kernel_stats(cfdgpu_handle *h, int kind, int64_t *launches, double *total_ms, double *total_bytes);
 
+/* ---- batched stepping of independent instances -----------------------
+ * No counterpart in the reference (one mesh per process).  A batch owns one
+ * handle per instance (each with its own mesh, control and solver options)
+ * and a pool of host threads that step the instances concurrently on the
+ * current device, largest first.  Each instance computes exactly what its
+ * own handle would alone.  For many concurrent streams to reach the GPU
+ * separately, set CUDA_DEVICE_MAX_CONNECTIONS (e.g. 32) before the process
+ * creates its CUDA context. */
+#define CFDGPU_BATCH_MAX 4096
+#define CFDGPU_BATCH_MAX_THREADS 128
+typedef struct cfdgpu_batch cfdgpu_batch;
+/* count instances, arrays of count structs; on failure *out may still be set
+ * (read cfdgpu_batch_last_error, then cfdgpu_batch_destroy) */
+int cfdgpu_batch_create(int count, const cfdgpu_mesh *meshes, const cfdgpu_control *ctrls,
+                        const cfdgpu_solver_opts *opts, cfdgpu_batch **out);
+int cfdgpu_batch_destroy(cfdgpu_batch *b);
+const char *cfdgpu_batch_last_error(cfdgpu_batch *b);
+int cfdgpu_batch_size(cfdgpu_batch *b);
+/* instance i's handle (get/set solution, history, timers...); owned by the batch */
+cfdgpu_handle *cfdgpu_batch_handle(cfdgpu_batch *b, int i);
+/* concurrency: host threads stepping instances at once; chunk: Arnoldi steps
+ * per CUDA graph between host polls (1..64).  (0, 0) = autotune: the next
+ * batch steps each try one candidate pair, scored by wall time per GMRES
+ * iteration, and the best is kept.  Results do not depend on either. */
+int cfdgpu_batch_set_schedule(cfdgpu_batch *b, int concurrency, int chunk);
+int cfdgpu_batch_get_schedule(cfdgpu_batch *b, int *concurrency, int *chunk, int *tuned);
+/* one time step of every instance: timeNow/timeFact per instance (count
+ * values each); stats and latency_ms (host wall time of each instance's
+ * step) per instance.  Returns the first failing instance's code. */
+int cfdgpu_batch_step(cfdgpu_batch *b, const double *timeNow, const double *timeFact, cfdgpu_step_stats *stats,
+                      double *latency_ms);
+
 #ifdef __cplusplus
 }
 #endif

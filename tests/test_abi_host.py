@@ -17,7 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "cfdgpu.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*\*?\s*(cfdgpu_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*|cfdgpu_handle \*)\s*\*?\s*(cfdgpu_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -149,3 +149,20 @@ def test_create_fails_loudly_without_device():
     with pytest.raises(_lib.CfdGpuError) as ei:
         _lib.Handle(m, c)
     assert ei.value.code in (_lib.ENODEV, _lib.ECUDA)
+
+
+def test_batch_create_fails_loudly_without_device():
+    """The batch runtime has no CPU fallback either: without a GPU the first
+    instance's create error comes back with the instance named."""
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("GPU present")
+    cases = [(meshgen.cavity2d(n), meshgen.control_for(5, 0.05, 0.01)) for n in (4, 6)]
+    with pytest.raises(_lib.CfdGpuError) as ei:
+        _lib.Batch(cases)
+    assert ei.value.code in (_lib.ENODEV, _lib.ECUDA)
+    assert "instance 0" in str(ei.value)
