@@ -9,7 +9,9 @@
 // sleep (blocking-sync events) so that dozens of threads can share a few cores.
 //
 // Schedule: instances are taken largest first (longest-processing-time
-// order); `concurrency` threads take part; `chunk` is the number of Arnoldi
+// order) and their streams get priorities by size (largest highest), so the
+// longest dependent kernel chains are not slowed by the small instances;
+// `concurrency` threads take part; `chunk` is the number of Arnoldi
 // steps per graph between host polls.  With both set to 0 the batch
 // autotunes: the first batch steps try candidate (concurrency, chunk) pairs,
 // one pair per step, scored by wall time per GMRES iteration of the step, and
@@ -145,6 +147,21 @@ int cfdgpu_batch_create(int count, const cfdgpu_mesh *meshes, const cfdgpu_contr
   b->order.resize(count);
   for (int i = 0; i < count; i++) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(), [&](int a, int c) { return b->work[a] > b->work[c]; });
+  // stream priorities by size: the largest systems have the longest chains
+  // of dependent Arnoldi kernels, so their kernels go first and the small
+  // instances fill the gaps
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  const int levels = least - greatest + 1;
+  for (int k = 0; k < count && levels > 1; k++) {
+    const int prio = greatest + (int)((int64_t)k * levels / count);
+    const int rc = cfdgpu::set_stream_priority(b->h[b->order[k]], prio);
+    if (rc) {
+      b->err = "stream priority";
+      *out = b;
+      return rc;
+    }
+  }
   b->rc.assign(count, 0);
   const int nthreads = std::min(count, CFDGPU_BATCH_MAX_THREADS);
   for (int t = 0; t < nthreads; t++) b->workers.emplace_back(worker_main, b, t);

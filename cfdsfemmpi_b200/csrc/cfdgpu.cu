@@ -768,6 +768,17 @@ int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk)
   return 0;
 }
 
+int set_stream_priority(cfdgpu_handle *h, int priority)
+{
+  if (!h) return CFDGPU_EINVAL;
+  cudaStream_t s2 = nullptr;
+  CK(cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, priority));
+  CK(cudaStreamSynchronize(h->stream));
+  cudaStreamDestroy(h->stream);
+  h->stream = s2;
+  return 0;
+}
+
 int handle_work(cfdgpu_handle *h, double *dofs, double *blocks)
 {
   if (!h) return CFDGPU_EINVAL;

@@ -25,6 +25,11 @@ int handle_graph(cfdgpu_handle *h, GraphView *out);
 // on either (Arnoldi kernels after convergence are no-ops)
 int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk);
 
+// replace the handle's stream by a non-blocking stream of the given
+// priority (lower value = higher priority); cached Arnoldi graphs follow the
+// priority of the stream they are launched into
+int set_stream_priority(cfdgpu_handle *h, int priority);
+
 // size of a handle's system: dofs and BSR blocks (work estimate)
 int handle_work(cfdgpu_handle *h, double *dofs, double *blocks);
 
