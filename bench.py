@@ -230,11 +230,16 @@ def run_ours(args, world, rank, local):
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     achieved = (by / nl) / (ms / nl * 1e-3) / 1e9 if nl else None
+    # DRAM traffic per launch: the ratio of ncu-measured DRAM bytes to
+    # algorithmic bytes for this kernel kind and workload (profiles/), times
+    # this run's algorithmic bytes per launch
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and nl:
         try:
-            traffic = json.load(open(tpath)).get(args.workload, {}).get(dom)
+            ent = json.load(open(tpath)).get(args.workload, {}).get(dom)
+            if ent:
+                traffic = ent["dram_bytes_per_algorithmic_byte"] * by / nl
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_src,
