@@ -567,8 +567,7 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
       if ((r = arnoldi(j))) return r;
       const int pi = prof_begin(h, CFDGPU_KIND_ORTHO, (2.0 * j + 3.0) * (double)sizeof(VT) * n);
       dim3 g2(ntiles, (j + 1 + MDOT_KC - 1) / MDOT_KC);
-      gmres_mdot<VT><<<g2, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga.partial);
-      gmres_mdot_reduce<<<(j + 1 + 7) / 8, 256, 0, h->stream>>>(ntiles, j, st, K.ga.partial, K.ga.H, K.ga.sigma);
+      gmres_mdot<VT><<<g2, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga);
       gmres_maxpy_norm<VT><<<mtiles, ORTHO_THREADS, 0, h->stream>>>(nchunk, V, ldv, j, st, K.ga);
       prof_end(h, pi);
     }
@@ -600,10 +599,10 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
           h->launches = before;   // counted when the graph runs
         }
         CK(cudaGraphLaunch(ex, h->stream));
-        h->launches += 4 * nk;
+        h->launches += 3 * nk;
       } else {
         if ((rc = enqueue_chunk(j0))) return rc;
-        h->launches += 4 * nk;
+        h->launches += 3 * nk;
       }
       const int cidx = (j0 / CH) & 1;
       CK(cudaMemcpyAsync(&h->h_gst[cidx], st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
@@ -899,6 +898,9 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = dalloc(h, &h->ga32.y, (size_t)h->m32))) return rc;
     const int64_t nt32 = (h->ldv / 4 + ORTHO_THREADS - 1) / ORTHO_THREADS + h->ldv / 4 / MAXPY_SPAN + 1;
     if ((rc = dalloc(h, &h->ga32.partial, (size_t)(h->m32 + 1) * std::max<int64_t>(nt32, RED_BLOCKS)))) return rc;
+    if ((rc = dalloc(h, &h->ga32.coef, (size_t)h->m32 + 1))) return rc;
+    if ((rc = dalloc(h, &h->ga32.kcount, (size_t)h->m32 / MDOT_KC + 2))) return rc;
+    CK(cudaMemset(h->ga32.kcount, 0, sizeof(unsigned int) * (h->m32 / MDOT_KC + 2)));
   } else {
     if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
     CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
@@ -918,6 +920,9 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     const int64_t ntiles = (h->ldv / 2 + ORTHO_THREADS - 1) / ORTHO_THREADS + h->ldv / 2 / MAXPY_SPAN + 1;
     if ((rc = dalloc(h, &h->ga.partial, (size_t)(h->m + 1) * std::max<int64_t>(ntiles, RED_BLOCKS)))) return rc;
   }
+  if ((rc = dalloc(h, &h->ga.coef, (size_t)h->m + 1))) return rc;
+  if ((rc = dalloc(h, &h->ga.kcount, (size_t)h->m / MDOT_KC + 2))) return rc;
+  CK(cudaMemset(h->ga.kcount, 0, sizeof(unsigned int) * (h->m / MDOT_KC + 2)));
   if ((rc = dalloc(h, &h->red_partial, (size_t)RED_BLOCKS))) return rc;
   if ((rc = dalloc(h, &h->red_partial2, (size_t)5 * RED_BLOCKS))) return rc;
   if ((rc = dalloc(h, &h->red_counter, 1))) return rc;

@@ -43,6 +43,8 @@ struct GmresArrays {
   double *grs;     // m+1
   double *y;       // m
   double *partial; // scratch for reductions: (m+1) * ntiles doubles
+  double *coef;    // m+1: H(k, j) * sigma[k], the update coefficients of Arnoldi step j
+  unsigned int *kcount;   // m/8+1 arrival counters of the multi-dot's k-groups (zero between launches)
 };
 
 __device__ __forceinline__ int ksp_converged(GmresState *s, int n_its, double rnorm)
@@ -465,13 +467,18 @@ __device__ __forceinline__ int64_t hidx(int r, int c, int m) { return (int64_t)c
 constexpr int ORTHO_THREADS = 256;
 constexpr int MDOT_KC = 8;          // basis vectors per CTA in the multi-dot
 
-// Classical Gram-Schmidt dot products, pass 1: per column tile partial sums
-// of <w, V_k> for a chunk of MDOT_KC vectors.  grid (ntiles, ceil((j+1)/KC)).
+// Classical Gram-Schmidt dot products <w, V_k> for a group of MDOT_KC
+// vectors per grid row: grid (ntiles, ceil((j+1)/KC)).  Every CTA stores its
+// tile partial sums; the last CTA to arrive in a grid row adds that row's
+// partials (one warp per k, lanes strided over the tiles, then a fixed
+// shuffle tree) and stores H(k, j) = sigma_k <w, V_k> and the update
+// coefficient H(k, j) sigma_k.
 template <typename VT>
 __global__ void __launch_bounds__(ORTHO_THREADS)
 gmres_mdot(int64_t nchunk, const VT *__restrict__ V, int64_t ldv, int j, const GmresState *__restrict__ st,
-           double *__restrict__ partial)
+           GmresArrays ga)
 {
+  double *__restrict__ partial = ga.partial;
   if (!st->active || st->it != j) return;
   constexpr int E = Chunk<VT>::E;
   __shared__ double sh[MDOT_KC][ORTHO_THREADS / 32];
@@ -512,24 +519,21 @@ gmres_mdot(int64_t nchunk, const VT *__restrict__ V, int64_t ldv, int j, const G
     for (int w2 = 0; w2 < ORTHO_THREADS / 32; w2++) t += sh[threadIdx.x][w2];
     partial[(int64_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = t;
   }
-}
-
-// pass 2: one warp per k sums the tile partials in a fixed order and scales by
-// the stored vector's sigma -> H(k, j) = <w, sigma_k V_k>
-__global__ void gmres_mdot_reduce(int ntiles, int j, const GmresState *__restrict__ st,
-                                  const double *__restrict__ partial, double *__restrict__ H,
-                                  const double *__restrict__ sigma)
-{
-  if (!st->active || st->it != j) return;
-  const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (k > j) return;
-  const double *pp = partial + (int64_t)k * ntiles;
-  double t = 0.0;
-  for (int b = lane; b < ntiles; b += 32) t += pp[b];
+  if (last_block(&ga.kcount[blockIdx.y], gridDim.x)) {
+    if (wid < nk) {
+      const int k = k0 + wid;
+      const double *pp = partial + (int64_t)k * gridDim.x;
+      double t = 0.0;
+      for (unsigned int b = lane; b < gridDim.x; b += 32) t += __ldcg(pp + b);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-  if (lane == 0) H[hidx(k, j, st->m)] = sigma[k] * t;
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) {
+        const double hkj = ga.sigma[k] * t;
+        ga.H[hidx(k, j, st->m)] = hkj;
+        ga.coef[k] = hkj * ga.sigma[k];
+      }
+    }
+  }
 }
 
 // w -= sum_k h_k sigma_k V_k, then ||w||^2 partials.  A CTA covers
@@ -548,17 +552,22 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
 {
   if (!st->active || st->it != j) return;
   constexpr int E = Chunk<VT>::E;
-  __shared__ double hk[1024];
   __shared__ double sh[ORTHO_THREADS / 32];
   __shared__ double qs[ORTHO_THREADS / MAXPY_CHUNKS][E][MAXPY_SPAN];
   const int m = st->m;
-  for (int k = threadIdx.x; k <= j; k += blockDim.x) hk[k] = ga.H[hidx(k, j, m)] * ga.sigma[k];
-  __syncthreads();
+  // coefficients H(k, j) sigma_k (written by the multi-dot), read as
+  // warp-uniform broadcasts inside the loop
+  const double *__restrict__ hk = ga.coef;
   VT *w = V + (int64_t)(j + 1) * ldv;
   const int lp = threadIdx.x % MAXPY_CHUNKS;
   const int quarter = threadIdx.x / MAXPY_CHUNKS;
   const int64_t p0 = (int64_t)blockIdx.x * MAXPY_SPAN + lp;
   const int64_t p1 = p0 + MAXPY_CHUNKS;
+  // the chunk of w this thread finishes (quarters 0 and 1), loaded early
+  const int cfin = lp + (quarter & 1) * MAXPY_CHUNKS;
+  const int64_t pfin = (int64_t)blockIdx.x * MAXPY_SPAN + cfin;
+  double wfin[E];
+  if (quarter < 2 && pfin < nchunk) Chunk<VT>::load(w + E * pfin, wfin);
   double a0[E], a1[E];
 #pragma unroll
   for (int e = 0; e < E; e++) { a0[e] = 0.0; a1[e] = 0.0; }
@@ -570,26 +579,28 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
     int k = quarter;
     for (; k + 4 <= j; k += 8) {
       double v0[E], v1[E], u0[E], u1[E];
+      const double c0 = __ldg(hk + k), c1 = __ldg(hk + k + 4);
       Chunk<VT>::load(b0 + (int64_t)k * ldv, v0);
       Chunk<VT>::load(b1 + (int64_t)k * ldv, u0);
       Chunk<VT>::load(b0 + (int64_t)(k + 4) * ldv, v1);
       Chunk<VT>::load(b1 + (int64_t)(k + 4) * ldv, u1);
 #pragma unroll
       for (int e = 0; e < E; e++) {
-        a0[e] = fma(hk[k], v0[e], a0[e]);
-        a1[e] = fma(hk[k], u0[e], a1[e]);
-        a0[e] = fma(hk[k + 4], v1[e], a0[e]);
-        a1[e] = fma(hk[k + 4], u1[e], a1[e]);
+        a0[e] = fma(c0, v0[e], a0[e]);
+        a1[e] = fma(c0, u0[e], a1[e]);
+        a0[e] = fma(c1, v1[e], a0[e]);
+        a1[e] = fma(c1, u1[e], a1[e]);
       }
     }
     for (; k <= j; k += 4) {
       double v0[E], u0[E];
+      const double c0 = __ldg(hk + k);
       Chunk<VT>::load(b0 + (int64_t)k * ldv, v0);
       Chunk<VT>::load(b1 + (int64_t)k * ldv, u0);
 #pragma unroll
       for (int e = 0; e < E; e++) {
-        a0[e] = fma(hk[k], v0[e], a0[e]);
-        a1[e] = fma(hk[k], u0[e], a1[e]);
+        a0[e] = fma(c0, v0[e], a0[e]);
+        a1[e] = fma(c0, u0[e], a1[e]);
       }
     }
   }
@@ -602,11 +613,12 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
   double s = 0.0;
   // quarter q < 2 finishes chunk lp + q*MAXPY_CHUNKS
   if (quarter < 2) {
-    const int c = lp + quarter * MAXPY_CHUNKS;
-    const int64_t p = (int64_t)blockIdx.x * MAXPY_SPAN + c;
+    const int c = cfin;
+    const int64_t p = pfin;
     if (p < nchunk) {
       double a[E];
-      Chunk<VT>::load(w + E * p, a);
+#pragma unroll
+      for (int e = 0; e < E; e++) a[e] = wfin[e];
 #pragma unroll
       for (int e = 0; e < E; e++) a[e] -= ((qs[0][e][c] + qs[1][e][c]) + (qs[2][e][c] + qs[3][e][c]));
       Chunk<VT>::store(w + E * p, a);
@@ -627,8 +639,7 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
     // stage column j of H and the stored rotations in shared memory (hk is
     // free again), so the serial rotation chain below runs from registers and
     // shared memory instead of global-memory round trips
-    __shared__ double rc[1024], rs[1024];
-    double *hc = hk;
+    __shared__ double rc[1024], rs[1024], hc[1024];
     const int it = j;
     for (int q = threadIdx.x; q <= it; q += blockDim.x) hc[q] = ga.H[hidx(q, it, m)];
     for (int q = threadIdx.x; q < it; q += blockDim.x) { rc[q] = ga.cs[q]; rs[q] = ga.sn[q]; }
