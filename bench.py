@@ -68,7 +68,7 @@ def parse():
     p.add_argument("--train-iters", type=int, default=3000)
     p.add_argument("--batch-count", type=int, default=64, help="batch: number of independent 2D cavities")
     p.add_argument("--batch-schedule", default="auto",
-                   help="batch: 'auto' (autotune during the warm-up steps) or 'C,K' (concurrency, chunk)")
+                   help="batch: 'auto' (autotune during the warm-up steps) or 'C,K,D' (concurrency, chunk, depth)")
     return p.parse_args()
 
 
@@ -498,7 +498,7 @@ def run_batch(args, world, rank, local):
     cases = meshgen.batch_cases(count=args.batch_count, seed=2024 + rank)
     pairs = [(m, c) for m, c, _, _ in cases]
     dt = pairs[0][1].dt
-    ntune = 12
+    ntune = 12        # autotuner candidates: concurrency (32, all) x chunk (4, 8) x depth (1, 2, 4)
     warm = max(args.warmup, ntune)
     steps = args.steps
     n = len(pairs)
@@ -536,8 +536,8 @@ def run_batch(args, world, rank, local):
     if args.batch_schedule == "auto":
         b.set_schedule(0, 0)
     else:
-        c, ch = (int(x) for x in args.batch_schedule.split(","))
-        b.set_schedule(c, ch)
+        c, ch, dp = (int(x) for x in args.batch_schedule.split(","))
+        b.set_schedule(c, ch, dp)
     for k in range(warm):
         b.step(times(k))
     sched = b.schedule()

@@ -139,9 +139,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_batch_size.argtypes = [vp]
     L.cfdgpu_batch_handle.argtypes = [vp, ip]
     L.cfdgpu_batch_handle.restype = vp
-    L.cfdgpu_batch_set_schedule.argtypes = [vp, ip, ip]
-    L.cfdgpu_batch_get_schedule.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                                            ctypes.POINTER(ctypes.c_int)]
+    L.cfdgpu_batch_set_schedule.argtypes = [vp, ip, ip, ip]
+    L.cfdgpu_batch_get_schedule.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 4
     L.cfdgpu_batch_step.argtypes = [vp, vp, vp, ctypes.POINTER(StepStats), vp]
     L.cfdgpu_launch_count.argtypes = [vp]
     L.cfdgpu_launch_count.restype = ctypes.c_int64
@@ -522,14 +521,14 @@ class Batch:
         if rc != 0:
             raise CfdGpuError(rc, self._L.cfdgpu_batch_last_error(self.b).decode())
 
-    def set_schedule(self, concurrency: int = 0, chunk: int = 0):
-        """(0, 0): autotune over the next batch steps."""
-        self._check(self._L.cfdgpu_batch_set_schedule(self.b, concurrency, chunk))
+    def set_schedule(self, concurrency: int = 0, chunk: int = 0, depth: int = 0):
+        """(0, 0, 0): autotune over the next batch steps."""
+        self._check(self._L.cfdgpu_batch_set_schedule(self.b, concurrency, chunk, depth))
 
     def schedule(self):
-        c, ch, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        self._check(self._L.cfdgpu_batch_get_schedule(self.b, ctypes.byref(c), ctypes.byref(ch), ctypes.byref(t)))
-        return {"concurrency": c.value, "chunk": ch.value, "tuned": bool(t.value)}
+        v = [ctypes.c_int() for _ in range(4)]
+        self._check(self._L.cfdgpu_batch_get_schedule(self.b, *[ctypes.byref(x) for x in v]))
+        return {"concurrency": v[0].value, "chunk": v[1].value, "depth": v[2].value, "tuned": bool(v[3].value)}
 
     def step(self, times):
         """One step of every instance at times[i] (ramp factor min(t, 1)).

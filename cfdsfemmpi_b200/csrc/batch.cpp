@@ -12,10 +12,13 @@
 // order) and their streams get priorities by size (largest highest), so the
 // longest dependent kernel chains are not slowed by the small instances;
 // `concurrency` threads take part; `chunk` is the number of Arnoldi
-// steps per graph between host polls.  With both set to 0 the batch
-// autotunes: the first batch steps try candidate (concurrency, chunk) pairs,
-// one pair per step, scored by wall time per GMRES iteration of the step, and
-// the best pair is kept for the rest of the run.  Neither knob changes any
+// steps per graph; `depth` the number of chunks a handle keeps enqueued
+// beyond the one whose state its host thread waits for (a sleeping thread
+// wakes up tens of microseconds after its event, so small instances need
+// more than one chunk in flight to keep their stream busy).  With all three
+// set to 0 the batch autotunes: the first batch steps try candidate
+// triples, one per step, scored by wall time per GMRES iteration of the
+// step, and the best is kept for the rest of the run.  No knob changes any
 // number an instance computes (kernels after GMRES convergence are no-ops and
 // every reduction has a fixed order), so each instance's results are bitwise
 // those of its own single-instance run.
@@ -42,12 +45,15 @@ struct cfdgpu_batch {
   std::vector<int> order;              // instance indices, largest system first
   std::vector<double> work;            // BSR blocks per instance
   // schedule
-  int concurrency = 0, chunk = 0;      // in use
+  struct Sched {
+    int concurrency, chunk, depth;
+  };
+  Sched cur{0, 0, 0};                  // in use
   bool autotune = true, tuned = false;
-  std::vector<std::pair<int, int>> candidates;
+  std::vector<Sched> candidates;
   size_t trial = 0;
   double best_cost = std::numeric_limits<double>::infinity();
-  std::pair<int, int> best{0, 0};
+  Sched best{0, 0, 0};
   std::vector<double> trial_cost;
   // worker pool
   std::vector<std::thread> workers;
@@ -78,7 +84,7 @@ void worker_main(cfdgpu_batch *b, int id)
       if (b->quit) return;
       seen = b->generation;
     }
-    if (id < b->concurrency) {
+    if (id < b->cur.concurrency) {
       for (;;) {
         const int k = b->next.fetch_add(1);
         if (k >= (int)b->order.size()) break;
@@ -96,29 +102,26 @@ void worker_main(cfdgpu_batch *b, int id)
   }
 }
 
-int apply_schedule(cfdgpu_batch *b, int concurrency, int chunk)
+int apply_schedule(cfdgpu_batch *b, cfdgpu_batch::Sched s)
 {
   for (auto *h : b->h) {
-    const int rc = cfdgpu::set_host_schedule(h, true, chunk);
+    const int rc = cfdgpu::set_host_schedule(h, true, s.chunk, s.depth);
     if (rc) return rc;
   }
-  b->concurrency = concurrency;
-  b->chunk = chunk;
+  b->cur = s;
   return 0;
 }
 
 void make_candidates(cfdgpu_batch *b)
 {
   const int n = (int)b->h.size();
-  std::vector<int> cs;
-  for (int c : {8, 16, 32, 64, 128})
-    if (c < n) cs.push_back(c);
-  cs.push_back(std::min(n, (int)b->workers.size()));
-  std::sort(cs.begin(), cs.end());
+  const int all = std::min(n, (int)b->workers.size());
+  std::vector<int> cs = {std::min(32, all), all};
   cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
   b->candidates.clear();
-  for (int ch : {4, 8, 16})
-    for (int c : cs) b->candidates.emplace_back(c, ch);
+  for (int depth : {1, 2, 4})
+    for (int ch : {4, 8})
+      for (int c : cs) b->candidates.push_back({c, ch, depth});
 }
 
 }  // namespace
@@ -166,7 +169,7 @@ int cfdgpu_batch_create(int count, const cfdgpu_mesh *meshes, const cfdgpu_contr
   const int nthreads = std::min(count, CFDGPU_BATCH_MAX_THREADS);
   for (int t = 0; t < nthreads; t++) b->workers.emplace_back(worker_main, b, t);
   make_candidates(b);
-  const int rc = apply_schedule(b, b->candidates[0].first, b->candidates[0].second);
+  const int rc = apply_schedule(b, b->candidates[0]);
   *out = b;
   return rc;
 }
@@ -196,28 +199,30 @@ cfdgpu_handle *cfdgpu_batch_handle(cfdgpu_batch *b, int i)
   return b->h[i];
 }
 
-int cfdgpu_batch_set_schedule(cfdgpu_batch *b, int concurrency, int chunk)
+int cfdgpu_batch_set_schedule(cfdgpu_batch *b, int concurrency, int chunk, int depth)
 {
-  if (!b || concurrency < 0 || chunk < 0 || chunk > 64) return CFDGPU_EINVAL;
-  if (concurrency == 0 && chunk == 0) {
+  if (!b || concurrency < 0 || chunk < 0 || chunk > 64 || depth < 0 || depth > CFDGPU_BATCH_MAX_DEPTH)
+    return CFDGPU_EINVAL;
+  if (concurrency == 0 && chunk == 0 && depth == 0) {
     b->autotune = true;
     b->tuned = false;
     b->trial = 0;
     b->best_cost = std::numeric_limits<double>::infinity();
     b->trial_cost.clear();
-    return apply_schedule(b, b->candidates[0].first, b->candidates[0].second);
+    return apply_schedule(b, b->candidates[0]);
   }
-  if (concurrency == 0 || chunk == 0) return CFDGPU_EINVAL;
+  if (concurrency == 0 || chunk == 0 || depth == 0) return CFDGPU_EINVAL;
   b->autotune = false;
   b->tuned = true;
-  return apply_schedule(b, std::min(concurrency, (int)b->workers.size()), chunk);
+  return apply_schedule(b, {std::min(concurrency, (int)b->workers.size()), chunk, depth});
 }
 
-int cfdgpu_batch_get_schedule(cfdgpu_batch *b, int *concurrency, int *chunk, int *tuned)
+int cfdgpu_batch_get_schedule(cfdgpu_batch *b, int *concurrency, int *chunk, int *depth, int *tuned)
 {
   if (!b) return CFDGPU_EINVAL;
-  if (concurrency) *concurrency = b->concurrency;
-  if (chunk) *chunk = b->chunk;
+  if (concurrency) *concurrency = b->cur.concurrency;
+  if (chunk) *chunk = b->cur.chunk;
+  if (depth) *depth = b->cur.depth;
   if (tuned) *tuned = b->tuned ? 1 : 0;
   return 0;
 }
@@ -263,11 +268,11 @@ int cfdgpu_batch_step(cfdgpu_batch *b, const double *timeNow, const double *time
     }
     b->trial++;
     if (b->trial < b->candidates.size()) {
-      const int rc = apply_schedule(b, b->candidates[b->trial].first, b->candidates[b->trial].second);
+      const int rc = apply_schedule(b, b->candidates[b->trial]);
       if (rc) return rc;
     } else {
       b->tuned = true;
-      const int rc = apply_schedule(b, b->best.first, b->best.second);
+      const int rc = apply_schedule(b, b->best);
       if (rc) return rc;
     }
   }

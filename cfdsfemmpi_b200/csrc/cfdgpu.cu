@@ -85,9 +85,12 @@ struct cfdgpu_handle {
   double *h_scalar = nullptr;        // pinned host mirror
   GmresState *h_gst = nullptr;       // pinned
   bool assembled_K = false;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evw = nullptr;
+  static constexpr int MAX_DEPTH = 8;
+  cudaEvent_t evq[MAX_DEPTH + 1] = {};   // one per chunk in flight
+  cudaEvent_t evw = nullptr;
   bool blocking = false;   // host waits sleep (cudaEventBlockingSync) instead of spinning
   int chunk = 8;           // Arnoldi steps enqueued (and replayed as one graph) between host polls
+  int depth = 1;           // chunks enqueued beyond the one whose state the host waits for
   // learned initial guess
   cfdgpu_mpnn *guess = nullptr;
   int guess_mode = 0;
@@ -577,10 +580,12 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
     gmres_start<VT><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, V, st, K.ga);
     h->launches += 1;
     if ((rc = check_launch(h, "gmres_start"))) return rc;
-    // poll the device flag one chunk behind so the GPU stays fed
+    // poll the device flag `depth` chunks behind so the GPU stays fed; the
+    // chunks enqueued past convergence run as no-ops
     bool stop = false;
-    cudaEvent_t evs[2] = {h->ev0, h->ev1};
-    for (int j0 = 0; j0 < m && !stop; j0 += CH) {
+    const int D = h->depth, R = D + 1;
+    int c = 0;
+    for (int j0 = 0; j0 < m && !stop; j0 += CH, c++) {
       const int nk = std::min(m, j0 + CH) - j0;
       if (h->use_graphs && !h->prof) {
         std::vector<cudaGraphExec_t> &cache = K.graphs;
@@ -604,13 +609,13 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
         if ((rc = enqueue_chunk(j0))) return rc;
         h->launches += 3 * nk;
       }
-      const int cidx = (j0 / CH) & 1;
+      const int cidx = c % R;
       CK(cudaMemcpyAsync(&h->h_gst[cidx], st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
-      CK(cudaEventRecord(evs[cidx], h->stream));
-      // wait for the previous chunk's snapshot
-      if (j0 > 0) {
-        const int pidx = cidx ^ 1;
-        CK(cudaEventSynchronize(evs[pidx]));
+      CK(cudaEventRecord(h->evq[cidx], h->stream));
+      // wait for the snapshot taken `depth` chunks ago
+      if (c >= D) {
+        const int pidx = (c - D) % R;
+        CK(cudaEventSynchronize(h->evq[pidx]));
         if (!h->h_gst[pidx].active) stop = true;
       }
     }
@@ -619,9 +624,10 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
     gmres_update_x<VT><<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, V, ldv, st, K.ga, 1.0);
     h->launches += 1;
     if ((rc = check_launch(h, "gmres_build_soln"))) return rc;
-    CK(cudaMemcpyAsync(h->h_gst, st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
+    GmresState *fin = h->h_gst + cfdgpu_handle::MAX_DEPTH + 1;
+    CK(cudaMemcpyAsync(fin, st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
     if ((rc = host_wait(h))) return rc;
-    GmresState s = h->h_gst[0];
+    GmresState s = *fin;
     int reason = s.reason;
     if (reason == 0 && s.its >= max_it) reason = -3;   // KSP_DIVERGED_ITS
     if (reason != 0 || single_cycle) {
@@ -745,18 +751,22 @@ static int check_negjac(cfdgpu_handle *h)
 
 namespace cfdgpu {
 
-int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk)
+int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk, int depth)
 {
-  if (!h || chunk < 1 || chunk > 64) return CFDGPU_EINVAL;
+  if (!h || chunk < 1 || chunk > 64 || depth < 1 || depth > cfdgpu_handle::MAX_DEPTH) return CFDGPU_EINVAL;
   if (blocking != h->blocking) {
-    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    constexpr int NE = cfdgpu_handle::MAX_DEPTH + 2;
+    cudaEvent_t e[NE] = {};
     const unsigned flags = cudaEventDisableTiming | (blocking ? cudaEventBlockingSync : 0u);
     for (auto &x : e) CK(cudaEventCreateWithFlags(&x, flags));
     CK(cudaStreamSynchronize(h->stream));
-    cudaEventDestroy(h->ev0); cudaEventDestroy(h->ev1); cudaEventDestroy(h->evw);
-    h->ev0 = e[0]; h->ev1 = e[1]; h->evw = e[2];
+    for (auto &x : h->evq) cudaEventDestroy(x);
+    cudaEventDestroy(h->evw);
+    for (int i = 0; i < NE - 1; i++) h->evq[i] = e[i];
+    h->evw = e[NE - 1];
     h->blocking = blocking;
   }
+  h->depth = depth;
   if (chunk != h->chunk) {
     // the cached Arnoldi graphs hold chunk-length pieces of the cycle
     CK(cudaStreamSynchronize(h->stream));
@@ -838,8 +848,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   if (!msg.empty()) { h->err = msg; return CFDGPU_EINVAL; }
   const Topology &t = h->topo;
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  CK(cudaEventCreateWithFlags(&h->ev0, cudaEventDisableTiming));
-  CK(cudaEventCreateWithFlags(&h->ev1, cudaEventDisableTiming));
+  for (auto &e : h->evq) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->evw, cudaEventDisableTiming));
   int rc = 0;
   const int64_t n = h->n;
@@ -932,7 +941,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   CK(cudaMemset(h->negjac, 0, sizeof(int)));
   CK(cudaMemset(h->gst, 0, sizeof(GmresState)));
   CK(cudaMallocHost(&h->h_scalar, 8 * sizeof(double)));
-  CK(cudaMallocHost(&h->h_gst, 2 * sizeof(GmresState)));
+  CK(cudaMallocHost(&h->h_gst, (cfdgpu_handle::MAX_DEPTH + 2) * sizeof(GmresState)));
   CK(cudaDeviceSynchronize());
   h->timers[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return 0;
@@ -948,8 +957,8 @@ int cfdgpu_destroy(cfdgpu_handle *h)
   for (auto &e : h->pev) cudaEventDestroy(e);
   for (auto g : h->graphs64) if (g) cudaGraphExecDestroy(g);
   for (auto g : h->graphs32) if (g) cudaGraphExecDestroy(g);
-  if (h->ev0) cudaEventDestroy(h->ev0);
-  if (h->ev1) cudaEventDestroy(h->ev1);
+  for (auto &e : h->evq)
+    if (e) cudaEventDestroy(e);
   if (h->evw) cudaEventDestroy(h->evw);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;

@@ -20,10 +20,11 @@ struct GraphView {
 // device view of a handle's mesh graph
 int handle_graph(cfdgpu_handle *h, GraphView *out);
 
-// host-side scheduling of a handle's step: blocking (sleeping) host waits and
-// the number of Arnoldi steps per graph chunk (1..64); results do not depend
-// on either (Arnoldi kernels after convergence are no-ops)
-int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk);
+// host-side scheduling of a handle's step: blocking (sleeping) host waits,
+// the number of Arnoldi steps per graph chunk (1..64) and the number of
+// chunks in flight beyond the one the host waits for (1..8); results do not
+// depend on any of them (Arnoldi kernels after convergence are no-ops)
+int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk, int depth);
 
 // replace the handle's stream by a non-blocking stream of the given
 // priority (lower value = higher priority); cached Arnoldi graphs follow the

@@ -295,6 +295,7 @@ int cfdgpu_kernel_stats(cfdgpu_handle *h, int kind, int64_t *launches, double *t
  * creates its CUDA context. */
 #define CFDGPU_BATCH_MAX 4096
 #define CFDGPU_BATCH_MAX_THREADS 128
+#define CFDGPU_BATCH_MAX_DEPTH 8
 typedef struct cfdgpu_batch cfdgpu_batch;
 /* count instances, arrays of count structs; on failure *out may still be set
  * (read cfdgpu_batch_last_error, then cfdgpu_batch_destroy) */
@@ -306,11 +307,12 @@ int cfdgpu_batch_size(cfdgpu_batch *b);
 /* instance i's handle (get/set solution, history, timers...); owned by the batch */
 cfdgpu_handle *cfdgpu_batch_handle(cfdgpu_batch *b, int i);
 /* concurrency: host threads stepping instances at once; chunk: Arnoldi steps
- * per CUDA graph between host polls (1..64).  (0, 0) = autotune: the next
- * batch steps each try one candidate pair, scored by wall time per GMRES
- * iteration, and the best is kept.  Results do not depend on either. */
-int cfdgpu_batch_set_schedule(cfdgpu_batch *b, int concurrency, int chunk);
-int cfdgpu_batch_get_schedule(cfdgpu_batch *b, int *concurrency, int *chunk, int *tuned);
+ * per CUDA graph (1..64); depth: chunks each instance keeps enqueued beyond
+ * the one whose state its thread waits for (1..8).  (0, 0, 0) = autotune:
+ * the next batch steps each try one candidate, scored by wall time per GMRES
+ * iteration, and the best is kept.  Results do not depend on any of them. */
+int cfdgpu_batch_set_schedule(cfdgpu_batch *b, int concurrency, int chunk, int depth);
+int cfdgpu_batch_get_schedule(cfdgpu_batch *b, int *concurrency, int *chunk, int *depth, int *tuned);
 /* one time step of every instance: timeNow/timeFact per instance (count
  * values each); stats and latency_ms (host wall time of each instance's
  * step) per instance.  Returns the first failing instance's code. */

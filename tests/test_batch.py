@@ -31,7 +31,7 @@ def _alone(cases, steps):
     return out
 
 
-@pytest.mark.parametrize("schedule", [(0, 0), (2, 3), (1, 8)])
+@pytest.mark.parametrize("schedule", [(0, 0, 0), (2, 3, 1), (1, 8, 2), (6, 4, 4)])
 def test_batch_matches_single_instance_runs_bitwise(schedule):
     cases = _cases()
     steps = 6
@@ -55,11 +55,12 @@ def test_batch_matches_single_instance_runs_bitwise(schedule):
             assert a["newton_iters"] == r["newton_iters"] and a["ksp_its"] == r["ksp_its"], (i, k)
             assert a["norms"] == r["norms"], (i, k)
     assert all(np.all(l > 0) for l in lats)
-    if schedule == (0, 0):
-        # 6 instances: one concurrency candidate (6) times three chunk lengths
-        assert sched["tuned"] and sched["concurrency"] == 6 and sched["chunk"] in (4, 8, 16)
+    if schedule == (0, 0, 0):
+        # 6 instances: one concurrency candidate (6) x chunks (4, 8) x depths (1, 2, 4)
+        assert sched["tuned"] and sched["concurrency"] == 6 and sched["chunk"] in (4, 8)
+        assert sched["depth"] in (1, 2, 4)
     else:
-        assert sched == {"concurrency": schedule[0], "chunk": schedule[1], "tuned": True}
+        assert sched == {"concurrency": schedule[0], "chunk": schedule[1], "depth": schedule[2], "tuned": True}
 
 
 def test_batch_reports_the_failing_instance():
@@ -67,7 +68,7 @@ def test_batch_reports_the_failing_instance():
     fail with that instance's error; the others are unaffected."""
     cases = _cases()[:3]
     b = Batch(cases, restart=50, rtol=1e-10, pc="jacobi", max_it=1)
-    b.set_schedule(3, 8)
+    b.set_schedule(3, 8, 1)
     with pytest.raises(Exception) as e:
         b.step(np.full(3, 0.05))
     assert "instance 0" in str(e.value) and "KSP" in str(e.value)
