@@ -481,6 +481,14 @@ def run_guess(args, world, rank, local):
 # GMRES(50)+Jacobi at rtol 1e-10 (the 2D configuration) stalls on the larger
 # batch cavities (n >= 129 reach max_it); GMRES(400) + point-block Jacobi at
 # rtol 1e-8 converges every step in two Newton iterations
+def _hbm_peak():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
 BATCH_SOLVER = {"restart": 400, "rtol": 1e-8, "pc": "pbjacobi", "max_it": 20000}
 
 
@@ -545,12 +553,30 @@ def run_batch(args, world, rank, local):
     launches0 = sum(h.launch_count() for h in b.handles)
     clocks = ClockSampler(local)
     clocks.start()
-    lat_b, its_b = [], 0
+    # algorithmic HBM bytes of the Krylov work (the whole step's dominant
+    # cost): per Arnoldi step j of a cycle, SpMV with the point-block Jacobi
+    # epilogue B*b^2*8 + 4B + 4(N+1) + 2V + N*b^2*8 and Gram-Schmidt (2j+5)V
+    infos = [h.pattern_info() for h in b.handles]
+    m = BATCH_SOLVER["restart"]
+
+    def krylov_bytes(i, its):
+        pi = infos[i]
+        bb = pi.ndof * pi.ndof
+        V = 8.0 * pi.nNode * pi.ndof
+        spmv = pi.nnzb * bb * 8 + 4 * pi.nnzb + 4 * (pi.nNode + 1) + 2 * V + pi.nNode * bb * 8
+        full, rest = divmod(its, m)
+        js = full * (m * (m - 1)) + rest * (rest - 1)          # 2 * sum of j over the iterations
+        return its * spmv + (js + 5 * its) * V
+
+    lat_b, its_b, alg_bytes = [], 0, 0.0
     T0 = time.perf_counter()
     for k in range(warm, warm + steps):
         st, lat = b.step(times(k))
         lat_b.extend(lat.tolist())
         its_b += sum(sum(s.ksp_its[:s.newton_iters]) for s in st)
+        for i, s_ in enumerate(st):
+            for q in range(s_.newton_iters):
+                alg_bytes += krylov_bytes(i, s_.ksp_its[q])
     torch.cuda.synchronize()
     wall_b = time.perf_counter() - T0
     ck = clocks.stop()
@@ -573,6 +599,11 @@ def run_batch(args, world, rank, local):
                        "synchronisation", "l2": "inputs resident; no flush (the batch is the working set)",
                        "timed_steps": f"{warm + 1}..{warm + steps}", "parallelism": "single GPU, concurrent streams"},
             "latency_ms": {"p50": float(np.percentile(lat_b, 50)), "p99": float(np.percentile(lat_b, 99))},
+            "roofline": {"bound": "hbm", "kernel": "all Krylov kernels of all instances (SpMV + Gram-Schmidt)",
+                         "achieved": alg_bytes / wall_b / 1e9, "peak": _hbm_peak()[0], "peak_source": _hbm_peak()[1],
+                         "unit": "GB/s", "frac": alg_bytes / wall_b / 1e9 / _hbm_peak()[0], "traffic": None,
+                         "algorithmic_bytes_per_step": alg_bytes / steps,
+                         "one_by_one_achieved": alg_bytes / wall_seq / 1e9},
             "one_by_one": {"value": n * steps / wall_seq, "unit": "instance-steps/s",
                            "latency_ms": {"p50": float(np.percentile(lat_seq, 50)),
                                           "p99": float(np.percentile(lat_seq, 99))},

@@ -16,6 +16,12 @@ std::string build_topology(int nNode, int nElem, int npe, int ndof, const int32_
   if (nNode <= 0 || nElem <= 0) return "empty mesh";
   for (int64_t k = 0; k < (int64_t)nElem * npe; k++)
     if (conn[k] < 0 || conn[k] >= nNode) return "connectivity refers to a node outside [0, nNode)";
+  // a node listed twice in one element would make two lanes of the element
+  // kernel write the same matrix block at once
+  for (int e = 0; e < nElem; e++)
+    for (int a = 0; a < npe; a++)
+      for (int b = a + 1; b < npe; b++)
+        if (conn[(int64_t)e * npe + a] == conn[(int64_t)e * npe + b]) return "element with a repeated node";
 
   // node -> incident elements
   std::vector<int32_t> eptr(nNode + 1, 0);

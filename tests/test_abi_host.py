@@ -166,3 +166,30 @@ def test_batch_create_fails_loudly_without_device():
         _lib.Batch(cases)
     assert ei.value.code in (_lib.ENODEV, _lib.ECUDA)
     assert "instance 0" in str(ei.value)
+
+
+@pytest.mark.parametrize("case", ["empty", "node_out_of_range", "negative_node", "repeated_node", "bad_dbc_node",
+                                  "bad_dbc_dof"])
+def test_invalid_meshes_are_rejected(case):
+    """Bad input comes back as CFDGPU_EINVAL from the host set-up (the same
+    checks run in cfdgpu_create before anything reaches the device)."""
+    m = meshgen.cavity2d(3)
+    conn = m.conn.copy()
+    dbc = m.dbc.copy()
+    nNode = m.nNode
+    if case == "empty":
+        conn = conn[:0]
+    elif case == "node_out_of_range":
+        conn[2, 1] = nNode
+    elif case == "negative_node":
+        conn[0, 0] = -1
+    elif case == "repeated_node":
+        conn[1, 2] = conn[1, 0]
+    elif case == "bad_dbc_node":
+        dbc[0, 0] = nNode + 5
+    elif case == "bad_dbc_dof":
+        dbc[0, 1] = 3
+    bad = io.Mesh(ndim=2, npElem=4, coords=m.coords, conn=conn, dbc=dbc, output_nodes=np.zeros(0, np.int32))
+    with pytest.raises(_lib.CfdGpuError) as ei:
+        pattern_build(bad)
+    assert ei.value.code == _lib.EINVAL

@@ -338,3 +338,18 @@ def test_vtu_and_forces_output(golden_dir, tmp_path):
     assert np.allclose(d["pressure"], s[:, 2], atol=1e-6)
     lines = [l for l in open(str(tmp_path / "LDC2Dquad10-forces.dat")).read().split("\n") if l.strip()]
     assert len(lines) == 3 and lines[0].startswith("0.10000000000000")
+
+
+@pytest.mark.parametrize("kind", ["tri3", "tet4"])
+def test_tri3_tet4_time_steps_match_oracle(kind):
+    """Time stepping with the simplex elements (split cavity meshes), 3 steps:
+    GMRES(200)+pbjacobi at rtol 1e-12 against the oracle with a direct solve."""
+    mesh = MESHES[kind]()
+    ctrl = meshgen.control_for(3, 0.1, 0.01)
+    ref = oracle.OracleFEM(mesh, ctrl, solver="lu")
+    ref.solve()
+    s, stats = _run_gpu(mesh, ctrl, restart=200, rtol=1e-12, pc="pbjacobi")
+    rel = np.linalg.norm(s - ref.soln) / np.linalg.norm(ref.soln)
+    assert rel < 1e-8, rel
+    assert len(stats) == 3 and all(st["converged"] for st in stats)
+    assert [st["newton_iters"] for st in stats] == [len(st["norms"]) for st in ref.stats]
