@@ -67,6 +67,7 @@ def parse():
                    help="first training sample n (u_{n-1}, u_n -> u_{n+1}); 0 = two steps after the lid ramp")
     p.add_argument("--train-iters", type=int, default=3000)
     p.add_argument("--batch-count", type=int, default=64, help="batch: number of independent 2D cavities")
+    p.add_argument("--no-batch-mixed", action="store_true", help="batch: skip the mixed-precision batch arm")
     p.add_argument("--batch-schedule", default="auto",
                    help="batch: 'auto' (autotune during the warm-up steps) or 'C,K,D' (concurrency, chunk, depth)")
     return p.parse_args()
@@ -584,6 +585,34 @@ def run_batch(args, world, rank, local):
     launches = sum(h.launch_count() for h in b.handles) - launches0
     b.close()
     equal = sum(int(np.array_equal(a, c)) for a, c in zip(sol_b, sol_seq))
+
+    # the same batch in mixed precision (FP32 tangent + inner GMRES(100),
+    # FP64 refinement and Newton residual), same steps and schedule rule
+    mixed = None
+    if not args.no_batch_mixed:
+        bm = Batch(pairs, **dict(BATCH_SOLVER, precision="mixed", inner_restart=100, inner_rtol=1e-4,
+                                 max_it=40000))
+        bm.set_schedule(0, 0, 0)
+        for k in range(warm):
+            bm.step(times(k))
+        torch.cuda.synchronize()
+        T0 = time.perf_counter()
+        lat_m = []
+        for k in range(warm, warm + steps):
+            st, lat = bm.step(times(k))
+            lat_m.extend(lat.tolist())
+        torch.cuda.synchronize()
+        wall_m = time.perf_counter() - T0
+        sol_m = [h.get_solution() for h in bm.handles]
+        sched_m = bm.schedule()
+        bm.close()
+        dv = []
+        for a, c in zip(sol_m, sol_b):
+            a3, c3 = a.reshape(-1, 3), c.reshape(-1, 3)
+            dv.append(float(np.linalg.norm(a3[:, :2] - c3[:, :2]) / max(np.linalg.norm(c3[:, :2]), 1e-300)))
+        mixed = {"value": n * steps / wall_m, "unit": "instance-steps/s", "speedup_vs_one_by_one": wall_seq / wall_m,
+                 "latency_ms": {"p50": float(np.percentile(lat_m, 50)), "p99": float(np.percentile(lat_m, 99))},
+                 "schedule": sched_m, "max_velocity_rel_diff_vs_fp64_batch": max(dv)}
     wall_max = barrier_max(world, wall_b)
     value = world * n * steps / wall_max
     dofs = sum(m.nNode * m.ndof for m, _ in pairs)
@@ -617,6 +646,7 @@ def run_batch(args, world, rank, local):
                                  "Re": float(cases[int(lat_mat.sum(axis=0).argmax())][3]),
                                  "batch_step_over_bound": float(wall_b * 1e3 / steps / lat_mat.max(axis=1).mean())},
             "instances_bitwise_equal_to_one_by_one": f"{equal}/{n}", "gpu_launches": int(launches),
+            "mixed_precision_batch": mixed,
             "clocks": ck}
     return line
 

@@ -425,8 +425,10 @@ static int build_pc(cfdgpu_handle *h)
   const int pc = h->opts.pc_type;
   if (pc == CFDGPU_PC_NONE) return 0;
   const int g = (h->nNode + 127) / 128;
-  if (h->mixed) {
+  if (h->mixed && h->ndof == 4) {
     build_jacobi<4, float, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr32, h->dinv32, h->binv32, pc);
+  } else if (h->mixed) {
+    build_jacobi<3, float, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr32, h->dinv32, h->binv32, pc);
   } else if (h->ndof == 4) {
     build_jacobi<4, double, double><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr, h->dinv, h->binv, pc);
   } else {
@@ -484,13 +486,23 @@ static int spmv32_pc(cfdgpu_handle *h, const float *x, float *y, const GmresStat
 {
   const int pc = h->opts.pc_type;
   const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 0, 4, 4, pc));
-  const int grid = (int)((h->nNode * 32LL + 255) / 256);
-  if (pc == 0)
-    bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
-  else if (pc == 1)
-    bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
-  else
-    bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+  if (h->ndof == 4) {
+    const int grid = (int)((h->nNode * 32LL + 255) / 256);
+    if (pc == 0)
+      bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+    else if (pc == 1)
+      bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+    else
+      bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+  } else {
+    const int grid = (int)((h->n + 255) / 256);
+    if (pc == 0)
+      bsr_spmv_generic_f32<3, 0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+    else if (pc == 1)
+      bsr_spmv_generic_f32<3, 1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+    else
+      bsr_spmv_generic_f32<3, 2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+  }
   prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "bsr_spmv_f32");
@@ -687,7 +699,10 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
     // b32 = r64 / ||r64|| (the device norm lives in scalar[1])
     if ((rc = norm2_dev(h, h->r64, h->scalar + 1))) return rc;
     k_scale_to_f32<<<grid_for(n), 256, 0, h->stream>>>(n, h->r64, h->scalar + 1, h->b32);
-    pc_apply<4, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
+    if (h->ndof == 4)
+      pc_apply<4, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
+    else
+      pc_apply<3, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
     h->launches += 2;
     if ((rc = check_launch(h, "mixed_prepare"))) return rc;
     auto arn = [&](int j) {
@@ -704,9 +719,15 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
     LAUNCHED(h);
     {
       const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 1, 8, 4, 0));
-      const int grid = (int)((h->nNode * 32LL + 255) / 256);
-      bsr4_spmv<1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b, nullptr,
-                                                           nullptr, h->r64, nullptr, 0, nullptr);
+      if (h->ndof == 4) {
+        const int grid = (int)((h->nNode * 32LL + 255) / 256);
+        bsr4_spmv<1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b, nullptr,
+                                                             nullptr, h->r64, nullptr, 0, nullptr);
+      } else {
+        const int grid = (int)((h->n + 255) / 256);
+        bsr_spmv_generic<3, 1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b,
+                                                                      nullptr, nullptr, h->r64, nullptr, 0, nullptr);
+      }
       prof_end(h, pi);
       LAUNCHED(h);
       if ((rc = check_launch(h, "mixed_residual"))) return rc;
@@ -877,7 +898,6 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   }
   const size_t bb = (size_t)h->ndof * h->ndof;
   h->mixed = (h->opts.precision == CFDGPU_PREC_MIXED);
-  if (h->mixed && h->ndof != 4) { h->err = "mixed precision is built for the 4x4-block (3D) systems"; return CFDGPU_EINVAL; }
   // Krylov stride: a multiple of 512 entries, so every update CTA covers whole chunks
   h->ldv = (n + 511) / 512 * 512;
   if (h->mixed) {

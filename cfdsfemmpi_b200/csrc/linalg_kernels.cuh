@@ -244,6 +244,52 @@ __global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, 
   y[t] = v;
 }
 
+// The same for other block sizes (3x3 in 2D), FP32 blocks and vectors: one
+// thread per scalar row, FP32 accumulation as in the 4x4 FP32 kernel.
+template <int NB, int PC>
+__global__ void bsr_spmv_generic_f32(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
+                                     const float *__restrict__ val, const float *__restrict__ x,
+                                     const float *__restrict__ dinv, const float *__restrict__ binv,
+                                     float *__restrict__ y, const GmresState *__restrict__ st, int j,
+                                     const double *__restrict__ xscale)
+{
+  if (st && (!st->active || st->it != j)) return;
+  const float xs = xscale ? (float)xscale[0] : 1.f;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t node = t / NB;
+  const int row = (int)(t % NB);
+  if (node >= nrows) return;
+  const int kb0 = rowptr[node], kb1 = rowptr[node + 1];
+  if (PC == 2) {
+    float vv[NB];
+#pragma unroll
+    for (int rr = 0; rr < NB; rr++) {
+      float s = 0.f;
+      for (int kb = kb0; kb < kb1; kb++) {
+        const int c = colidx[kb];
+        const float *a = val + (int64_t)kb * NB * NB + rr * NB;
+#pragma unroll
+        for (int q = 0; q < NB; q++) s = fmaf(a[q], x[(int64_t)c * NB + q], s);
+      }
+      vv[rr] = xs * s;
+    }
+    float z = 0.f;
+#pragma unroll
+    for (int q = 0; q < NB; q++) z += binv[node * NB * NB + row * NB + q] * vv[q];
+    y[t] = z;
+    return;
+  }
+  float acc = 0.f;
+  for (int kb = kb0; kb < kb1; kb++) {
+    const int c = colidx[kb];
+    const float *a = val + (int64_t)kb * NB * NB + row * NB;
+#pragma unroll
+    for (int q = 0; q < NB; q++) acc = fmaf(a[q], x[(int64_t)c * NB + q], acc);
+  }
+  acc *= xs;
+  y[t] = (PC == 1) ? dinv[t] * acc : acc;
+}
+
 // z = M^-1 r (stand-alone preconditioner application)
 template <int NB, typename VT, typename PT>
 __global__ void pc_apply(int64_t n, int pc, const PT *__restrict__ dinv, const PT *__restrict__ binv,

@@ -278,6 +278,24 @@ def test_mixed_precision_path(n, steps):
     assert rel < 5e-2, rel
 
 
+def test_mixed_precision_path_2d():
+    """The mixed-precision path on 3x3 blocks (2D cavity 32x32, Re 1000,
+    dt 0.05, 8 steps): every step meets the absolute 1e-8 residual and the
+    velocity agrees with an FP64 run solved to rtol 1e-12 (the pressure
+    follows the same sensitivity bound as in 3D)."""
+    mesh = meshgen.cavity2d(32)
+    ctrl = meshgen.control_for(8, 0.05, 1e-3)
+    ref, _ = _run_gpu(mesh, ctrl, restart=400, rtol=1e-12, pc="pbjacobi", max_it=40000)
+    mix, st_mix = _run_gpu(mesh, ctrl, restart=400, pc="pbjacobi", precision="mixed", inner_restart=100,
+                           inner_rtol=1e-4, max_it=40000)
+    assert all(s["converged"] for s in st_mix), st_mix
+    assert all(s["norms"][-1] < 1e-8 for s in st_mix)
+    a, b = mix.reshape(-1, 3), ref.reshape(-1, 3)
+    dv = np.linalg.norm(a[:, :2] - b[:, :2]) / np.linalg.norm(b[:, :2])
+    rel = np.linalg.norm(mix - ref) / np.linalg.norm(ref)
+    assert dv < 1e-4 and rel < 5e-2, (dv, rel)
+
+
 @pytest.mark.parametrize("kind", list(MESHES))
 def test_gpu_tangent_matches_finite_difference(kind):
     """diffStiffTest analogue (src/base/StabFEM.cpp:581-706) on the GPU element
