@@ -91,6 +91,7 @@ GMRES_OPTIONS = {"-ksp_type": "gmres", "-ksp_gmres_restart": "50", "-pc_type": "
 # name -> (builder, control, options) for the configurations named by the
 # benchmark description.  The 2D and 3D cavities start from rest.
 CASES = {
+    "cylinder": lambda: (cylinder_ogrid(), control_for(3000, 0.1, 0.01), dict(GMRES_OPTIONS)),
     "ldc2d_10": lambda: (cavity2d(10), control_for(20, 0.1, 0.01), dict(GMRES_OPTIONS)),
     "ldc3d_32": lambda: (cavity3d(32), control_for(50, 0.1, 0.001), dict(GMRES_OPTIONS)),
     "ldc3d_115": lambda: (cavity3d(115), control_for(20, 0.1, 0.001), dict(GMRES_OPTIONS)),
@@ -99,6 +100,59 @@ CASES = {
 
 def case_hex(n: int, steps: int, mu: float = 0.001, dt: float = 0.1):
     return cavity3d(n), control_for(steps, dt, mu), dict(GMRES_OPTIONS)
+
+
+def _geometric_ratio(n: int, r0: float, r1: float, dr0: float) -> float:
+    """q with r0 + dr0 (q^n - 1)/(q - 1) = r1 (bisection)."""
+    lo, hi = 1.0 + 1e-12, 2.0
+    f = lambda q: r0 + dr0 * (q ** n - 1.0) / (q - 1.0) - r1
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(mid) > 0:
+            hi = mid
+        else:
+            lo = mid
+    return 0.5 * (lo + hi)
+
+
+def cylinder_ogrid(nt: int = 256, nr: int = 128, r_in: float = 0.5, r_out: float = 20.0,
+                   dr0: float = 0.005) -> Mesh:
+    """O-grid around a cylinder of diameter 2 r_in at the origin inside a
+    circle of radius r_out: nt quads around, nr quads outward with geometric
+    radial spacing starting at dr0.  Boundary conditions: no-slip on the
+    cylinder, inflow (1, 0) on the outer arc where x < 0, traction-free
+    (nothing prescribed) where x >= 0; no pressure pin (the free outflow fixes
+    the pressure level).  Nodes are numbered ring by ring (k outward), i
+    counter-clockwise from the +x axis."""
+    q = _geometric_ratio(nr, r_in, r_out, dr0)
+    r = r_in + dr0 * (q ** np.arange(nr + 1) - 1.0) / (q - 1.0)
+    r[-1] = r_out
+    th = 2.0 * np.pi * np.arange(nt) / nt
+    R, TH = np.meshgrid(r, th, indexing="ij")          # (nr+1, nt)
+    coords = np.stack([(R * np.cos(TH)).ravel(), (R * np.sin(TH)).ravel()], axis=1)
+    nid = lambda i, k: (i % nt) + nt * k
+    kk, ii = np.meshgrid(np.arange(nr), np.arange(nt), indexing="ij")
+    kk = kk.ravel(); ii = ii.ravel()
+    # (radial, then tangential) edge order: counter-clockwise in (x, y)
+    conn = np.stack([nid(ii, kk), nid(ii, kk + 1), nid(ii + 1, kk + 1), nid(ii + 1, kk)], axis=1).astype(np.int32)
+    rows = []
+    for i in range(nt):
+        rows += [(nid(i, 0), 0, 0.0), (nid(i, 0), 1, 0.0)]
+    for i in range(nt):
+        node = nid(i, nr)
+        if coords[node, 0] < 0.0:
+            rows += [(node, 0, 1.0), (node, 1, 0.0)]
+    dbc = np.array(rows, dtype=np.float64)
+    return Mesh(ndim=2, npElem=4, coords=coords, conn=conn, dbc=dbc, output_nodes=np.zeros(0, np.int32))
+
+
+def cylinder_initial_state(mesh: Mesh, amplitude: float = 1e-3, seed: int = 12345) -> np.ndarray:
+    """Rest state with the transverse velocity perturbed by seeded uniform
+    noise of the given amplitude (triggers vortex shedding)."""
+    rng = np.random.default_rng(seed)
+    u = np.zeros((mesh.nNode, 3))
+    u[:, 1] = rng.uniform(-amplitude, amplitude, mesh.nNode)
+    return u.ravel()
 
 
 def batch_cases(count: int = 64, n_lo: int = 24, n_hi: int = 160, re_lo: float = 100.0, re_hi: float = 5000.0,
