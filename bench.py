@@ -586,6 +586,30 @@ def run_batch(args, world, rank, local):
     b.close()
     equal = sum(int(np.array_equal(a, c)) for a, c in zip(sol_b, sol_seq))
 
+    # the same batch with the min-residual extrapolation guess (FP64)
+    bx = Batch(pairs, guess="extrapolation", **BATCH_SOLVER)
+    bx.set_schedule(0, 0, 0)
+    for k in range(warm):
+        bx.step(times(k))
+    torch.cuda.synchronize()
+    T0 = time.perf_counter()
+    lat_x, its_x = [], 0
+    for k in range(warm, warm + steps):
+        st, lat = bx.step(times(k))
+        lat_x.extend(lat.tolist())
+        its_x += sum(sum(s.ksp_its[:s.newton_iters]) for s in st)
+    torch.cuda.synchronize()
+    wall_x = time.perf_counter() - T0
+    sol_x = [h.get_solution() for h in bx.handles]
+    bx.close()
+    dvx = []
+    for a, c in zip(sol_x, sol_b):
+        a3, c3 = a.reshape(-1, 3), c.reshape(-1, 3)
+        dvx.append(float(np.linalg.norm(a3[:, :2] - c3[:, :2]) / max(np.linalg.norm(c3[:, :2]), 1e-300)))
+    extrap = {"value": n * steps / wall_x, "unit": "instance-steps/s", "speedup_vs_one_by_one": wall_seq / wall_x,
+              "latency_ms": {"p50": float(np.percentile(lat_x, 50)), "p99": float(np.percentile(lat_x, 99))},
+              "gmres_iters": int(its_x), "max_velocity_rel_diff_vs_constant_predictor": max(dvx)}
+
     # the same batch in mixed precision (FP32 tangent + inner GMRES(100),
     # FP64 refinement and Newton residual), same steps and schedule rule
     mixed = None
@@ -646,6 +670,7 @@ def run_batch(args, world, rank, local):
                                  "Re": float(cases[int(lat_mat.sum(axis=0).argmax())][3]),
                                  "batch_step_over_bound": float(wall_b * 1e3 / steps / lat_mat.max(axis=1).mean())},
             "instances_bitwise_equal_to_one_by_one": f"{equal}/{n}", "gpu_launches": int(launches),
+            "extrapolation_guess_batch": extrap,
             "mixed_precision_batch": mixed,
             "clocks": ck}
     return line

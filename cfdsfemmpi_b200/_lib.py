@@ -489,7 +489,7 @@ class Batch:
     (io.Mesh, io.Control) pair with the same solver keywords) stepped
     concurrently on the current device."""
 
-    def __init__(self, cases, **solver_kw):
+    def __init__(self, cases, guess: str = "constant", **solver_kw):
         L = load()
         self._L = L
         self.b = ctypes.c_void_p()
@@ -513,6 +513,11 @@ class Batch:
             raise CfdGpuError(rc, msg)
         self.handles = [Handle._borrow(L.cfdgpu_batch_handle(self.b, i), mesh, self)
                         for i, (mesh, _) in enumerate(self.cases)]
+        if guess == "extrapolation":
+            for h in self.handles:
+                h.set_guess_mode(("extrapolation",))
+        elif guess != "constant":
+            raise ValueError(f"guess must be 'constant' or 'extrapolation', not {guess!r}")
 
     def __len__(self):
         return len(self.cases)
