@@ -159,7 +159,8 @@ def barrier_max(world, value):
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.barrier()
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
