@@ -65,3 +65,27 @@ def test_cli_runs_with_gmres_options(golden_dir, tmp_path):
     assert "Program is successful" in r.stdout
     assert "GMRES(50) pc=jacobi" in r.stdout
     assert "Convergence in" in r.stdout
+
+
+@pytest.mark.gpu
+def test_kat_with_extrapolation_guess_and_cli_options(golden_dir, tmp_path):
+    """The library's own option keys through the C++ driver: the min-residual
+    extrapolation guess still reproduces the shipped 10x10 solution (the guess
+    only changes where Newton starts), and the fully-implicit formulation and
+    bad option values are accepted or rejected as documented."""
+    assert _built()
+    mesh, ctrl, opts, ref = _copy_case(golden_dir, tmp_path)
+    with open(opts, "a") as f:
+        f.write("\n-gpu_guess extrapolation\n")
+    r = subprocess.run([os.path.join(BIN, "test-ldc-stru"), mesh, ctrl, opts, ref], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "Result matches" in r.stdout
+    fi = tmp_path / "fi.dat"
+    fi.write_text("-ksp_type gmres\n-ksp_gmres_restart 50\n-pc_type jacobi\n-ksp_rtol 1.e-10\n"
+                  "-gpu_formulation fully_implicit\n")
+    r = subprocess.run([os.path.join(BIN, "cfdsfemmpi"), mesh, ctrl, str(fi)], capture_output=True, text=True)
+    assert r.returncode == 0 and "Program is successful" in r.stdout, r.stderr[-2000:]
+    bad = tmp_path / "bad.dat"
+    bad.write_text("-gpu_formulation sideways\n")
+    r = subprocess.run([os.path.join(BIN, "cfdsfemmpi"), mesh, ctrl, str(bad)], capture_output=True, text=True)
+    assert r.returncode != 0 and "-gpu_formulation must be" in r.stderr
