@@ -66,6 +66,10 @@ def parse():
     p.add_argument("--train-first", type=int, default=0,
                    help="first training sample n (u_{n-1}, u_n -> u_{n+1}); 0 = two steps after the lid ramp")
     p.add_argument("--train-iters", type=int, default=3000)
+    p.add_argument("--newton-rtol", type=float, default=0.0,
+                   help="surrogate/extrapolation: extra relative Newton test for the mixed-precision variants "
+                        "(||F|| <= r ||F_0||, F_0 the constant predictor's iteration-0 residual); 0 = the 1e-8 "
+                        "absolute test only")
     p.add_argument("--batch-count", type=int, default=64, help="batch: number of independent 2D cavities")
     p.add_argument("--no-batch-mixed", action="store_true", help="batch: skip the mixed-precision batch arm")
     p.add_argument("--batch-schedule", default="auto",
@@ -401,6 +405,8 @@ def run_guess(args, world, rank, local):
         kw = dict(opts)
         if prec == "mixed":
             kw.update(precision="mixed", inner_restart=100, inner_rtol=1e-4, max_it=40000)
+            if args.newton_rtol > 0:
+                kw.update(newton_rtol=args.newton_rtol, newton_max_iter=30)
         if name == "reference_tight":
             kw.update(rtol=1e-12, max_it=40000)
         h = Handle(mesh, ctrl, **kw)

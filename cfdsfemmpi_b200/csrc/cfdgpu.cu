@@ -91,6 +91,7 @@ struct cfdgpu_handle {
   bool blocking = false;   // host waits sleep (cudaEventBlockingSync) instead of spinning
   int chunk = 8;           // Arnoldi steps enqueued (and replayed as one graph) between host polls
   int depth = 1;           // chunks enqueued beyond the one whose state the host waits for
+  double newton_target = 1e-8;   // this step's Newton stopping residual (absolute, and relative when asked)
   // learned initial guess
   cfdgpu_mpnn *guess = nullptr;
   int guess_mode = 0;
@@ -417,6 +418,7 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
     h->assembled_K = true;
   }
 
+
   return 0;
 }
 
@@ -676,8 +678,9 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
 // GMRES(m_inner) cycle (FP32 matrix, FP32 Krylov basis, FP32 preconditioner;
 // FP64 dot products and Hessenberg) to the inner tolerance,
 // x64 += ||r64|| * d, r64 = b - A32 x64 accumulated in FP64.
-// Stops when ||r64|| <= max(refine_rtol*||b||, 0.1*newton_tol) or after max
-// passes: the linear solve is not carried below the nonlinear tolerance, and
+// Stops when ||r64|| <= max(refine_rtol*||b||, 0.1*T) or after max passes,
+// T the step's Newton stopping residual (newton_tol, or the relative target
+// when newton_rtol is set): the linear solve is not carried below it, and
 // the Newton loop's FP64 residual (element kernels in FP64) decides whether
 // the step has converged and corrects the FP32 rounding of the tangent.
 static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *passes_out,
@@ -689,7 +692,7 @@ static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_ou
   CK(cudaMemcpyAsync(h->r64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
   double bnorm = 0.0;
   if ((rc = norm2(h, b, &bnorm))) return rc;
-  const double target = std::max(h->refine_rtol * bnorm, 0.1 * h->ctrl.newton_tol);
+  const double target = std::max(h->refine_rtol * bnorm, 0.1 * h->newton_target);
   int total = 0, passes = 0, reason = 2;
   double rn = bnorm;
   Krylov<float> K(h->graphs32);
@@ -897,6 +900,10 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     CK(cudaMemset(*v, 0, sizeof(double) * n));
   }
   const size_t bb = (size_t)h->ndof * h->ndof;
+  if (h->opts.precision != CFDGPU_PREC_FP64 && h->opts.precision != CFDGPU_PREC_MIXED) {
+    h->err = "unknown precision mode";
+    return CFDGPU_EINVAL;
+  }
   h->mixed = (h->opts.precision == CFDGPU_PREC_MIXED);
   // Krylov stride: a multiple of 512 entries, so every update CTA covers whole chunks
   h->ldv = (n + 511) / 512 * 512;
@@ -1127,8 +1134,15 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     stats->norms[iter] = norm;
     stats->newton_iters = iter + 1;
     // the reference's absolute test (StabFEM2.cpp:749); with newton_rtol > 0
-    // the residual must also have dropped by that factor from iteration 0
-    if (norm < h->ctrl.newton_tol && (h->opts.newton_rtol <= 0.0 || norm <= h->opts.newton_rtol * stats->norms[0])) {
+    // the residual must also have dropped by that factor from the
+    // iteration-0 residual of the constant predictor (the reference's start,
+    // so that a better initial guess does not tighten the test)
+    if (iter == 0) {
+      const double fref = (stats->plain_norm > 0.0) ? stats->plain_norm : norm;
+      h->newton_target = (h->opts.newton_rtol > 0.0) ? std::min(h->ctrl.newton_tol, h->opts.newton_rtol * fref)
+                                                      : h->ctrl.newton_tol;
+    }
+    if (norm < h->ctrl.newton_tol && norm <= h->newton_target) {
       stats->converged = 1;
       break;
     }

@@ -94,8 +94,10 @@ typedef struct cfdgpu_solver_opts {
   int inner_restart;        /* mixed mode: FP32 inner GMRES restart (0: 100) */
   double inner_rtol;        /* mixed mode: inner relative tolerance per refinement pass (0: 1e-4) */
   int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
-  double refine_rtol;       /* mixed mode: refinement target ||b - A32 x|| <= max(refine_rtol ||b||, newton_tol/10) (0: 1e-10) */
-  double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0|| (0: off, the reference's test only) */
+  double refine_rtol;       /* mixed mode: refinement target ||b - A32 x|| <= max(refine_rtol ||b||, T/10), T the
+                               step's Newton target below (0: 1e-10) */
+  double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0||, F_0 the iteration-0
+                               residual of the constant predictor (0: off, the reference's test only) */
   int formulation;          /* CFDGPU_FORM_*: element routine (0: the reference's active semi-implicit one) */
 } cfdgpu_solver_opts;
 
