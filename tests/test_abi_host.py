@@ -219,3 +219,29 @@ def test_cylinder_ogrid_matches_its_description():
     assert not np.any(d[:, 1] == 2)
     u0 = meshgen.cylinder_initial_state(m)
     assert np.all(u0.reshape(-1, 3)[:, [0, 2]] == 0) and 0 < np.abs(u0).max() <= 1e-3
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_pattern_matches_oracle_on_renumbered_meshes(seed):
+    """Ragged numbering: the cavity meshes with nodes and elements in random
+    order (and a pressure pin moved with them) give the oracle's free-dof
+    numbering, scalar pattern and colouring, bit for bit."""
+    rng = np.random.default_rng(seed)
+    for base in (meshgen.cavity2d(6), meshgen.cavity3d(3)):
+        perm = rng.permutation(base.nNode)          # old -> new node id
+        eorder = rng.permutation(base.nElem)
+        coords = np.empty_like(base.coords)
+        coords[perm] = base.coords
+        conn = perm[base.conn[eorder]].astype(np.int32)
+        dbc = base.dbc.copy()
+        dbc[:, 0] = perm[dbc[:, 0].astype(int)]
+        mesh = io.Mesh(ndim=base.ndim, npElem=base.npElem, coords=coords, conn=conn, dbc=dbc,
+                       output_nodes=np.zeros(0, np.int32))
+        d = pattern_build(mesh)
+        ref = oracle.OracleFEM(mesh, io.Control(), solver="lu")
+        assert np.array_equal(d["dofmap"], ref.dofmap)
+        rp, ci = scalar_pattern_from_blocks(d, mesh.ndof)
+        assert np.array_equal(rp, ref.rowptr) and np.array_equal(ci, ref.colidx)
+        col = np.zeros(mesh.nElem, np.int32)
+        nc = oracle.lib().orc_color(mesh.nNode, mesh.nElem, mesh.npElem, np.ascontiguousarray(mesh.conn, np.int32), col)
+        assert nc == d["info"].ncolors and np.array_equal(col, d["color"])

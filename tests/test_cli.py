@@ -89,3 +89,12 @@ def test_kat_with_extrapolation_guess_and_cli_options(golden_dir, tmp_path):
     bad.write_text("-gpu_formulation sideways\n")
     r = subprocess.run([os.path.join(BIN, "cfdsfemmpi"), mesh, ctrl, str(bad)], capture_output=True, text=True)
     assert r.returncode != 0 and "-gpu_formulation must be" in r.stderr
+
+
+def test_cli_reports_missing_input_files(tmp_path):
+    """Input errors come back before any device work, with the file named."""
+    assert _built()
+    r = subprocess.run([os.path.join(BIN, "cfdsfemmpi"), str(tmp_path / "nomesh"), str(tmp_path / "noctrl"),
+                        str(tmp_path / "noopts")], capture_output=True, text=True)
+    assert r.returncode != 0
+    assert "nomesh" in (r.stdout + r.stderr)
