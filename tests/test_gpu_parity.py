@@ -371,3 +371,50 @@ def test_tri3_tet4_time_steps_match_oracle(kind):
     assert rel < 1e-8, rel
     assert len(stats) == 3 and all(st["converged"] for st in stats)
     assert [st["newton_iters"] for st in stats] == [len(st["norms"]) for st in ref.stats]
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_tiny_meshes_match_oracle(n):
+    """Edge sizes: 1x1, 2x2 and 3x3 quad cavities (almost every dof prescribed;
+    the 1x1 case leaves only three pressures free) through the whole step."""
+    mesh = meshgen.cavity2d(n)
+    ctrl = meshgen.control_for(3, 0.1, 0.01)
+    ref = oracle.OracleFEM(mesh, ctrl, solver="lu")
+    ref.solve()
+    s, stats = _run_gpu(mesh, ctrl, restart=50, rtol=1e-12, pc="jacobi")
+    assert all(st["converged"] for st in stats)
+    err = np.linalg.norm(s - ref.soln) / max(np.linalg.norm(ref.soln), 1e-300)
+    assert err < 1e-8, err
+
+
+def test_single_hex_and_tet_elements():
+    """One hex8 (all nodes on the boundary) and one tet4: element matrices
+    against the oracle and a converged step."""
+    for mesh in (meshgen.cavity3d(1), _tri_tet("tet")):
+        if mesh.npElem == 4:
+            mesh = io.Mesh(ndim=3, npElem=4, coords=mesh.coords, conn=mesh.conn[:1], dbc=mesh.dbc,
+                           output_nodes=np.zeros(0, np.int32))
+            used = np.unique(mesh.conn)
+            remap = -np.ones(mesh.nNode, np.int64)
+            remap[used] = np.arange(len(used))
+            keep = np.isin(mesh.dbc[:, 0].astype(int), used)
+            dbc = mesh.dbc[keep].copy()
+            dbc[:, 0] = remap[dbc[:, 0].astype(int)]
+            mesh = io.Mesh(ndim=3, npElem=4, coords=mesh.coords[used], conn=remap[mesh.conn].astype(np.int32),
+                           dbc=dbc, output_nodes=np.zeros(0, np.int32))
+        ctrl = meshgen.control_for(2, 0.1, 0.01)
+        h = Handle(mesh, ctrl, restart=50, rtol=1e-12, pc="jacobi")
+        prev, cur, dot = _random_state(mesh.nNode * mesh.ndof, 5)
+        h.set_element_state(prev, cur, dot)
+        K, F = h.element_matrices(np.arange(mesh.nElem, dtype=np.int32))
+        td = oracle.time_params(2, 0.0, 0.1)
+        nodes = mesh.conn[0]
+        g = (nodes[:, None] * mesh.ndof + np.arange(mesh.ndof)).ravel()
+        Kr, Fr, _, _ = oracle.element(mesh.elem_type, mesh.coords[nodes], prev[g], cur[g], dot[g], ctrl.elem_data(), td)
+        assert np.abs(K[0] - Kr).max() <= 1e-13 * np.abs(Kr).max()
+        h.close()
+        ref = oracle.OracleFEM(mesh, ctrl, solver="lu")
+        ref.solve()
+        s, stats = _run_gpu(mesh, ctrl, restart=50, rtol=1e-12, pc="jacobi")
+        assert all(st["converged"] for st in stats)
+        assert np.linalg.norm(s - ref.soln) <= 1e-8 * max(np.linalg.norm(ref.soln), 1e-30)
