@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                    help="mixed: FP32 tangent storage and FP32 inner GMRES(100) with FP64 refinement")
-    p.add_argument("--method", default="plain", choices=["plain", "surrogate", "extrapolation", "batch"],
+    p.add_argument("--method", default="plain", choices=["plain", "surrogate", "extrapolation", "batch", "kernels"],
                    help="surrogate / extrapolation: run the plain solve for --train-steps, then time the "
                         "following steps from that state with mixed precision and the learned (surrogate) or "
                         "min-residual extrapolation initial guess; the line also carries every other variant "
@@ -71,6 +71,10 @@ def parse():
                         "(||F|| <= r ||F_0||, F_0 the constant predictor's iteration-0 residual); 0 = the 1e-8 "
                         "absolute test only")
     p.add_argument("--batch-count", type=int, default=64, help="batch: number of independent 2D cavities")
+    p.add_argument("--kernel-restart", type=int, default=40,
+                   help="kernels: GMRES restart of the bounded profiling case")
+    p.add_argument("--kernel-its", type=int, default=40,
+                   help="kernels: GMRES iterations of the bounded profiling case")
     p.add_argument("--no-batch-mixed", action="store_true", help="batch: skip the mixed-precision batch arm")
     p.add_argument("--batch-schedule", default="auto",
                    help="batch: 'auto' (autotune during the warm-up steps) or 'C,K,D' (concurrency, chunk, depth)")
@@ -683,6 +687,40 @@ def run_batch(args, world, rank, local):
     return line
 
 
+def run_kernels(args, local):
+    """A bounded case for profiling the hot kernels in isolation: the
+    workload's mesh, one tangent assembly (iteration-0 semantics) on a seeded
+    random state, and exactly --kernel-its GMRES iterations with restart
+    --kernel-restart on a seeded right-hand side, so a profiler sees the
+    element kernels, the BSR SpMV with its preconditioner and the Gram-Schmidt
+    kernels at realistic sizes and the run ends by itself.  Prints one JSON
+    line (not a benchmark value)."""
+    import numpy as np
+    import torch
+    from cfdsfemmpi_b200 import Handle, meshgen
+
+    torch.cuda.set_device(local)
+    n_side, _, opts = WORKLOADS[args.workload]
+    mesh, ctrl, _ = meshgen.case_hex(n_side, 2)
+    kw = dict(opts, restart=args.kernel_restart, rtol=1e-30, max_it=args.kernel_its)
+    h = Handle(mesh, ctrl, **kw)
+    rng = np.random.default_rng(0)
+    n = mesh.nNode * mesh.ndof
+    prev = 0.1 * rng.standard_normal(n)
+    h.set_element_state(prev, prev, np.zeros(n))
+    t0 = time.perf_counter()
+    h.assemble_export(0, want_values=False)
+    b = rng.standard_normal(n)
+    b[h.export_pattern()["fixed_dofs"]] = 0.0
+    x, its, reason = h.solve_export(b)
+    dt = time.perf_counter() - t0
+    line = {"method": "kernels", "workload": args.workload, "nodes": mesh.nNode, "pc": kw["pc"],
+            "restart": args.kernel_restart, "its": its, "reason": reason, "seconds": dt,
+            "launches": h.launch_count()}
+    h.close()
+    return line
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -697,7 +735,9 @@ def main():
         # CUDA context is created)
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     world, rank, local = dist_setup(args)
-    if args.method == "batch":
+    if args.method == "kernels":
+        line = run_kernels(args, local)
+    elif args.method == "batch":
         line = run_batch(args, world, rank, local)
     elif args.method in ("surrogate", "extrapolation"):
         line = run_guess(args, world, rank, local)

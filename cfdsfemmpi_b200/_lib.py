@@ -348,8 +348,13 @@ class Handle:
         d["info"] = pi
         return d
 
-    def assemble_export(self, it: int = 0):
+    def assemble_export(self, it: int = 0, want_values: bool = True):
+        """Assemble the tangent and RHS of the current state; with
+        want_values=False nothing is copied back (both returned as None)."""
         pi = self.pattern_info()
+        if not want_values:
+            self._check(self._L.cfdgpu_assemble_export(self.h, it, None, None))
+            return None, None
         vals = np.zeros(pi.nnzb * pi.ndof * pi.ndof)
         rhs = np.zeros(self.n)
         self._check(self._L.cfdgpu_assemble_export(self.h, it, _ptr(vals), _ptr(rhs)))

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1424,7 +1425,14 @@ int cfdgpu_kernel_stats(cfdgpu_handle *h, int kind, int64_t *launches, double *t
 //
 // Host code must not pass g_noalloc_scratch itself to a kernel: on the host that
 // name is a stand-in, not a device address.  The device address is looked up
-// once per device with cudaGetSymbolAddress and cached.
+// with cudaGetSymbolAddress, with the device current, and cached per device
+// under a mutex (two host threads making their first call on one device do not
+// race on the cache).  Calls made outside stream capture look the address up
+// again, so a cache entry left stale by cudaDeviceReset (which unloads the
+// module and may place the array elsewhere on the next load) is replaced
+// before it is used; a call made while its stream is being captured uses the
+// cached address, which is why the first call on a device must come before any
+// capture.
 namespace {
 constexpr int64_t NOALLOC_MAX_N = int64_t(1) << 21;          // residual entries (nNode*ndof)
 constexpr int64_t NOALLOC_WORDS = NOALLOC_MAX_N + RED_BLOCKS + 32;
@@ -1434,14 +1442,17 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_WORDS];
 
 static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+static std::mutex g_noalloc_mu;
 
-// Device address of the scratch array on the current device (set up once per
-// device, with that device current).
-static int noalloc_scratch(double **out)
+// Device address of the scratch array on the current device.
+static int noalloc_scratch(cudaStream_t s, double **out)
 {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CFDGPU_ENODEV;
-  if (!g_noalloc_ptr[dev]) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return CFDGPU_ECUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (cap == cudaStreamCaptureStatusNone || !g_noalloc_ptr[dev]) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return CFDGPU_ECUDA;
     g_noalloc_ptr[dev] = (double *)p;
@@ -1450,18 +1461,24 @@ static int noalloc_scratch(double **out)
   return 0;
 }
 
+static inline bool aligned_to(const void *p, uintptr_t a) { return ((uintptr_t)p % a) == 0; }
+
 extern "C" int cfdgpu_residual_norm_noalloc(int nNode, int ndof, const int32_t *d_rowptr, const int32_t *d_colidx,
                                             const double *d_val, const double *d_x, const double *d_b,
                                             double *d_norm, void *stream)
 {
   if (nNode <= 0 || (ndof != 3 && ndof != 4) || !d_rowptr || !d_colidx || !d_val || !d_x || !d_b || !d_norm)
     return CFDGPU_EINVAL;
+  // the 4x4 kernel reads blocks and x with 16-byte loads
+  if (!aligned_to(d_rowptr, 4) || !aligned_to(d_colidx, 4) || !aligned_to(d_val, 16) || !aligned_to(d_x, 16) ||
+      !aligned_to(d_b, 16) || !aligned_to(d_norm, 8))
+    return CFDGPU_EINVAL;
   const int64_t n = (int64_t)nNode * ndof;
   if (n > NOALLOC_MAX_N) return CFDGPU_ETOOBIG;
-  double *scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
-  if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
+  double *scratch = nullptr;
+  int rc = noalloc_scratch(s, &scratch);
+  if (rc) return rc;
   double *r = scratch;                                            // residual, n doubles
   double *partial = scratch + NOALLOC_MAX_N;                      // RED_BLOCKS doubles
   unsigned int *counter = (unsigned int *)(scratch + NOALLOC_MAX_N + RED_BLOCKS);

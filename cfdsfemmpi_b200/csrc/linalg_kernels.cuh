@@ -379,7 +379,7 @@ norm2_kernel(int64_t n, const double *__restrict__ x, double *__restrict__ parti
   if (last_block(counter, gridDim.x)) {
     if (threadIdx.x == 0) {
       double t = 0.0;
-      for (unsigned int k = 0; k < gridDim.x; k++) t += partial[k];
+      for (unsigned int k = 0; k < gridDim.x; k++) t += __ldcg(partial + k);
       out[0] = sqrt(t);
     }
   }
@@ -432,7 +432,7 @@ minres_dots(int64_t n, const double *__restrict__ a, const double *__restrict__ 
   if (last_block(counter, gridDim.x)) {
     if (threadIdx.x == 0) {
       double t0 = 0.0, t1 = 0.0;
-      for (unsigned int k = 0; k < gridDim.x; k++) { t0 += partial[2 * k]; t1 += partial[2 * k + 1]; }
+      for (unsigned int k = 0; k < gridDim.x; k++) { t0 += __ldcg(partial + 2 * k); t1 += __ldcg(partial + 2 * k + 1); }
       out[0] = t0;
       out[1] = t1;
     }
@@ -463,7 +463,7 @@ minres_dots2(int64_t n, const double *__restrict__ a, const double *__restrict__
   if (last_block(counter, gridDim.x)) {
     if (threadIdx.x < 5) {
       double t = 0.0;
-      for (unsigned int k = 0; k < gridDim.x; k++) t += partial[5 * k + threadIdx.x];
+      for (unsigned int k = 0; k < gridDim.x; k++) t += __ldcg(partial + 5 * k + threadIdx.x);
       out[threadIdx.x] = t;
     }
   }
@@ -485,7 +485,7 @@ gmres_start(int64_t n, const VT *__restrict__ v0, GmresState *st, GmresArrays ga
   if (last_block(&st->counter, gridDim.x)) {
     if (threadIdx.x == 0) {
       double t = 0.0;
-      for (unsigned int k = 0; k < gridDim.x; k++) t += ga.partial[k];
+      for (unsigned int k = 0; k < gridDim.x; k++) t += __ldcg(ga.partial + k);
       const double res = sqrt(t);
       st->res = res;
       st->it = 0;
@@ -680,7 +680,7 @@ gmres_maxpy_norm(int64_t nchunk, VT *__restrict__ V, int64_t ldv, int j, GmresSt
   if (threadIdx.x == 0) ga.partial[blockIdx.x] = s;
   if (last_block(&st->counter, gridDim.x)) {
     double t = 0.0;
-    for (unsigned int b = threadIdx.x; b < gridDim.x; b += ORTHO_THREADS) t += ga.partial[b];
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += ORTHO_THREADS) t += __ldcg(ga.partial + b);
     t = block_sum<ORTHO_THREADS>(t, sh);
     // stage column j of H and the stored rotations in shared memory (hk is
     // free again), so the serial rotation chain below runs from registers and

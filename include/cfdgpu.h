@@ -214,14 +214,20 @@ int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, dou
  * values in nodal blocks of ndof x ndof, row-major) and device vectors x, b
  * (nNode*ndof); the kernel writes ||b - A x||_2 to the device double d_norm,
  * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
- * ndof is 3 or 4.  Scratch lives in a fixed array inside the library (16 MiB,
- * held by every GPU that loads the library until exit); nNode*ndof above
- * 2,097,152 returns CFDGPU_ETOOBIG.  The call allocates nothing.  Its first
- * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (different streams, or different host threads
- * on one device) race and must be serialised by the caller.  This entry point
- * has no counterpart in the reference. */
+ * ndof is 3 or 4.  Alignment: d_val, d_x and d_b 16 bytes, d_norm 8 bytes,
+ * d_rowptr and d_colidx 4 bytes (the 4x4 kernel reads 16-byte vectors);
+ * other pointers return CFDGPU_EINVAL before any work is enqueued.  Scratch
+ * lives in a fixed array inside the library (16 MiB, held by every GPU that
+ * loads the library until exit); nNode*ndof above 2,097,152 returns
+ * CFDGPU_ETOOBIG.  The call allocates nothing.  Its first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress, with the device
+ * current) and should come before any stream capture; later calls outside
+ * capture look it up again, so the address stays valid after a
+ * cudaDeviceReset, while calls during capture use the address found by the
+ * last call outside capture.  All calls share the array: calls that overlap
+ * on the GPU (different streams, or different host threads on one device)
+ * race and must be serialised by the caller.  This entry point has no
+ * counterpart in the reference. */
 int cfdgpu_residual_norm_noalloc(int nNode, int ndof, const int32_t *d_rowptr, const int32_t *d_colidx,
                                  const double *d_val, const double *d_x, const double *d_b, double *d_norm,
                                  void *stream);
