@@ -21,9 +21,10 @@
  *   - free-dof pattern  src/base/StabFEM2.cpp:57-81, 192-227
  *   - Krylov solve: PETSc 3.10.5 KSPGMRES with classical Gram-Schmidt (no
  *     refinement), left preconditioning, preconditioned-residual norm,
- *     x0 = 0, and KSPConvergedDefault; PC "jacobi" (inverse diagonal).  PETSc
- *     is a third-party dependency that is not part of the reference tree; the
- *     algorithm below is its published one, called from SolverPetsc.cpp:253.
+ *     x0 = 0, and KSPConvergedDefault; PC "jacobi" (inverse diagonal); KSPBCGS;
+ *     PCBJACOBI with ILU(k) blocks.  PETSc is a third-party dependency that is
+ *     not part of the reference tree; the algorithms below are its published
+ *     ones, called from SolverPetsc.cpp:253.
  *
  * Build: oracle/Makefile (gcc -O2 -ffp-contract=off -fopenmp).
  */
@@ -804,6 +805,251 @@ static int small_inverse(int b, double *A)
   return 0;
 }
 
+/* ---------------- block Jacobi with ILU(k) blocks ----------------
+ *
+ * PETSc's PCBJACOBI with sub-KSP preonly and sub-PC ILU(levels), the
+ * preconditioner of the reference's iterative option files
+ * (input/petsc_options_gmres.dat:2-5, input/petsc_options_bcgs.dat:2-5, read
+ * through SolverPetsc.cpp:101,111).  PETSc is not part of the reference tree;
+ * this restates its published algorithm: the matrix is cut into diagonal
+ * blocks of contiguous rows (one per MPI rank in the reference, or the
+ * -pc_bjacobi_blocks count), couplings between blocks are dropped, and each
+ * block gets an incomplete LU factorisation in natural ordering with
+ * level-of-fill k (MatILUFactorSymbolic_SeqAIJ: lev(i,j) = min over pivots p
+ * of lev(i,p) + lev(p,j) + 1, entries of A at level 0, fill kept while
+ * lev <= k) followed by row-oriented numeric elimination
+ * (MatLUFactorNumeric_SeqAIJ: for row i, for each pivot p < i in the row's
+ * pattern in increasing order, l = w_p / u_pp, w_j -= l u_pj on the row's
+ * pattern).  Applying it solves L y = r (unit lower) and U z = y per block.
+ * The factors live in one CSR over all rows (block-local columns only).
+ * A very large level limit keeps all fill: the complete LU (-pc_type lu).
+ */
+typedef struct {
+  int n, nblk, levels;
+  int *blk;              /* nblk+1 row offsets */
+  int *fptr, *fcol;      /* factored pattern (sorted columns), n+1 / nnz */
+  int *fdiag;            /* position of the diagonal in each row */
+  double *fval;          /* L (unit, strict lower) and U (upper incl. diagonal) */
+  long nnz;
+  int zero_pivot_row;    /* first row with a zero pivot, -1 if none */
+  /* level sets: rows whose lower (upper) dependencies all lie in earlier
+   * sets; rows inside a set are independent, so the factorisation and the
+   * lower solve run set by set over lrows, the upper solve over urows, each
+   * row with the same arithmetic as in row order */
+  int nlev_l, nlev_u;
+  int *lptr, *lrows, *uptr, *urows;
+} orc_ilu_t;
+
+static orc_ilu_t g_ilu = {0};
+
+static void ilu_free(orc_ilu_t *f)
+{
+  free(f->blk); free(f->fptr); free(f->fcol); free(f->fdiag); free(f->fval);
+  free(f->lptr); free(f->lrows); free(f->uptr); free(f->urows);
+  memset(f, 0, sizeof(*f));
+}
+
+/* group rows by level: lev[] per row -> (ptr[nlev+1], rows[n]), row order
+ * inside a level */
+static int level_sets(int n, const int *lev, int **ptr_out, int **rows_out)
+{
+  int nlev = 0;
+  for (int i = 0; i < n; i++) if (lev[i] + 1 > nlev) nlev = lev[i] + 1;
+  int *ptr = calloc((size_t)nlev + 1, sizeof(int));
+  int *rows = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; i++) ptr[lev[i] + 1]++;
+  for (int k = 0; k < nlev; k++) ptr[k + 1] += ptr[k];
+  int *fill = calloc((size_t)nlev + 1, sizeof(int));
+  for (int i = 0; i < n; i++) rows[ptr[lev[i]] + fill[lev[i]]++] = i;
+  free(fill);
+  *ptr_out = ptr; *rows_out = rows;
+  return nlev;
+}
+
+/* Symbolic ILU(levels) of the diagonal blocks of the CSR (rowptr, colidx),
+ * blocks given as nblk+1 row offsets.  Returns nnz of the factors. */
+long orc_ilu_symbolic(int n, const int *rowptr, const int *colidx, int nblk, const int *blk, int levels)
+{
+  ilu_free(&g_ilu);
+  orc_ilu_t *f = &g_ilu;
+  f->n = n; f->nblk = nblk; f->levels = levels; f->zero_pivot_row = -1;
+  f->blk = malloc(sizeof(int) * (nblk + 1));
+  memcpy(f->blk, blk, sizeof(int) * (nblk + 1));
+  long cap = (long)rowptr[n] + 16;
+  int *col = malloc(sizeof(int) * cap);
+  int *lev = malloc(sizeof(int) * cap);      /* level of each stored entry */
+  int *ptr = malloc(sizeof(int) * (n + 1));
+  int *dg = malloc(sizeof(int) * (n > 0 ? n : 1));
+  int *next = malloc(sizeof(int) * (n + 1)); /* sorted linked list over columns, n = end marker */
+  int *lv = malloc(sizeof(int) * (n > 0 ? n : 1));
+  long nnz = 0;
+  ptr[0] = 0;
+  for (int b = 0; b < nblk; b++) {
+    const int r0 = blk[b], r1 = blk[b + 1];
+    for (int i = r0; i < r1; i++) {
+      /* row i of A inside the block, level 0 */
+      int head = n, tail = -1;
+      for (int k = rowptr[i]; k < rowptr[i + 1]; k++) {
+        int c = colidx[k];
+        if (c < r0 || c >= r1) continue;
+        lv[c] = 0;
+        if (tail < 0) head = c; else next[tail] = c;
+        tail = c;
+      }
+      if (tail >= 0) next[tail] = n;
+      /* eliminate pivots p < i in increasing order */
+      for (int p = head; p < i; p = next[p]) {
+        const int lp = lv[p];
+        if (lp + 1 > levels) continue;
+        int ins = p;   /* list position to search from: U columns of row p are > p, ascending */
+        for (long q = dg[p] + 1; q < ptr[p + 1]; q++) {
+          const int j = col[q];
+          const int l = lp + lev[q] + 1;
+          if (l > levels) continue;
+          while (next[ins] < j) ins = next[ins];
+          if (next[ins] == j) { if (l < lv[j]) lv[j] = l; }
+          else { next[j] = next[ins]; next[ins] = j; lv[j] = l; }
+          ins = j;
+        }
+      }
+      /* store row i */
+      long cnt = 0;
+      for (int c = head; c < n; c = next[c]) cnt++;
+      if (nnz + cnt > cap) {
+        while (nnz + cnt > cap) cap *= 2;
+        col = realloc(col, sizeof(int) * cap);
+        lev = realloc(lev, sizeof(int) * cap);
+      }
+      dg[i] = -1;
+      for (int c = head; c < n; c = next[c]) {
+        if (c == i) dg[i] = (int)nnz;
+        col[nnz] = c; lev[nnz] = lv[c]; nnz++;
+      }
+      ptr[i + 1] = (int)nnz;
+    }
+  }
+  free(next); free(lv); free(lev);
+  f->fptr = ptr; f->fcol = col; f->fdiag = dg; f->nnz = nnz;
+  f->fval = calloc((size_t)(nnz > 0 ? nnz : 1), sizeof(double));
+  /* dependency levels of the factorisation / lower solve (ascending) and of
+   * the upper solve (descending) */
+  int *dl = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; i++) {
+    int d = 0;
+    for (int q = ptr[i]; q < dg[i]; q++) if (dl[col[q]] + 1 > d) d = dl[col[q]] + 1;
+    dl[i] = d;
+  }
+  f->nlev_l = level_sets(n, dl, &f->lptr, &f->lrows);
+  for (int i = n - 1; i >= 0; i--) {
+    int d = 0;
+    for (int q = dg[i] + 1; q < ptr[i + 1]; q++) if (dl[col[q]] + 1 > d) d = dl[col[q]] + 1;
+    dl[i] = d;
+  }
+  f->nlev_u = level_sets(n, dl, &f->uptr, &f->urows);
+  free(dl);
+  return nnz;
+}
+
+/* export the factored pattern (rowptr n+1, colidx nnz, diag n) */
+void orc_ilu_pattern(int *fptr, int *fcol, int *fdiag)
+{
+  const orc_ilu_t *f = &g_ilu;
+  if (fptr) memcpy(fptr, f->fptr, sizeof(int) * (f->n + 1));
+  if (fcol) memcpy(fcol, f->fcol, sizeof(int) * f->nnz);
+  if (fdiag) memcpy(fdiag, f->fdiag, sizeof(int) * f->n);
+}
+
+/* Numeric ILU of (rowptr, colidx, vals) on the symbolic pattern, level set by
+ * level set (rows of a set in parallel).  Returns 0, or -1 on a zero pivot
+ * (the reference's PETSc would stop with a zero-pivot error). */
+int orc_ilu_numeric(const int *rowptr, const int *colidx, const double *vals, int nthreads)
+{
+  orc_ilu_t *f = &g_ilu;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  const int n = f->n;
+  int *blk_of = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int b = 0; b < f->nblk; b++)
+    for (int i = f->blk[b]; i < f->blk[b + 1]; i++) blk_of[i] = b;
+  int bad = n;
+#pragma omp parallel
+  {
+    double *w = calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+    int mybad = n;
+    for (int k = 0; k < f->nlev_l; k++) {
+#pragma omp for schedule(static)
+      for (int t = f->lptr[k]; t < f->lptr[k + 1]; t++) {
+        const int i = f->lrows[t];
+        const int r0 = f->blk[blk_of[i]], r1 = f->blk[blk_of[i] + 1];
+        for (int q = f->fptr[i]; q < f->fptr[i + 1]; q++) w[f->fcol[q]] = 0.0;
+        for (int kk = rowptr[i]; kk < rowptr[i + 1]; kk++) {
+          int c = colidx[kk];
+          if (c >= r0 && c < r1) w[c] = vals[kk];
+        }
+        for (int q = f->fptr[i]; q < f->fdiag[i]; q++) {
+          const int p = f->fcol[q];
+          const double l = w[p] / f->fval[f->fdiag[p]];
+          w[p] = l;
+          if (l != 0.0)
+            for (int u = f->fdiag[p] + 1; u < f->fptr[p + 1]; u++) w[f->fcol[u]] -= l * f->fval[u];
+        }
+        for (int q = f->fptr[i]; q < f->fptr[i + 1]; q++) f->fval[q] = w[f->fcol[q]];
+        if (f->fdiag[i] < 0 || f->fval[f->fdiag[i]] == 0.0) { if (i < mybad) mybad = i; }
+      }
+    }
+    free(w);
+#pragma omp critical
+    if (mybad < bad) bad = mybad;
+  }
+  free(blk_of);
+  f->zero_pivot_row = (bad < n) ? bad : -1;
+  return (bad < n) ? -1 : 0;
+}
+
+int orc_ilu_zero_pivot_row(void) { return g_ilu.zero_pivot_row; }
+
+/* z = (LU)^-1 r (every block at once: blocks share no dependencies) */
+static void ilu_apply(const double *r, double *z)
+{
+  const orc_ilu_t *f = &g_ilu;
+#pragma omp parallel
+  {
+    for (int k = 0; k < f->nlev_l; k++) {
+#pragma omp for schedule(static)
+      for (int t = f->lptr[k]; t < f->lptr[k + 1]; t++) {
+        const int i = f->lrows[t];
+        double s = r[i];
+        for (int q = f->fptr[i]; q < f->fdiag[i]; q++) s -= f->fval[q] * z[f->fcol[q]];
+        z[i] = s;
+      }
+    }
+    for (int k = 0; k < f->nlev_u; k++) {
+#pragma omp for schedule(static)
+      for (int t = f->uptr[k]; t < f->uptr[k + 1]; t++) {
+        const int i = f->urows[t];
+        double s = z[i];
+        for (int q = f->fdiag[i] + 1; q < f->fptr[i + 1]; q++) s -= f->fval[q] * z[f->fcol[q]];
+        z[i] = s / f->fval[f->fdiag[i]];
+      }
+    }
+  }
+}
+
+void orc_ilu_apply(const double *r, double *z, int nthreads)
+{
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  ilu_apply(r, z);
+}
+
+/* export the factor values (nnz) */
+void orc_ilu_values(double *v)
+{
+  memcpy(v, g_ilu.fval, sizeof(double) * g_ilu.nnz);
+}
+
 /* PETSc KSPConvergedReason values used here */
 #define R_ITERATING 0
 #define R_RTOL 2
@@ -816,6 +1062,7 @@ static int small_inverse(int b, double *A)
 
 static void pc_apply(int n, int pc, const double *dinv, const double *binv, const double *r, double *z)
 {
+  if (pc == 3) { ilu_apply(r, z); return; }
   if (pc != 2) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; i++) z[i] = dinv[i] * r[i];
@@ -990,6 +1237,105 @@ int orc_gmres(int n, const int *rowptr, const int *colidx, const double *vals, i
   if (its_out) *its_out = its;
   if (rnorm_out) *rnorm_out = res;
   free(dinv); free(binv); free(V); free(tmp); free(H); free(cc); free(ss); free(grs); free(nrs); free(hh);
+  return reason;
+}
+
+/*
+ * BiCGStab with left preconditioning (pc as in orc_gmres, 3 = the ILU set up
+ * by orc_ilu_symbolic/numeric), x0 = 0: PETSc 3.10 KSPSolve_BCGS, the solver
+ * of input/petsc_options_bcgs.dat:1 (third-party code, not in the reference
+ * tree; published algorithm restated).  The convergence test uses the
+ * preconditioned residual norm with KSPConvergedDefault; breakdowns (zero
+ * (v, rp), zero rho) end the solve with KSP_DIVERGED_BREAKDOWN.  Returns the
+ * KSPConvergedReason.
+ */
+int orc_bcgs(int n, const int *rowptr, const int *colidx, const double *vals, int pc,
+             const double *b, double *x, double rtol, double atol, double dtol,
+             int maxit, int *its_out, double *rnorm_out, int nthreads)
+{
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  double *dinv = malloc(sizeof(double) * n);
+  for (int r = 0; r < n; r++) {
+    double d = 0.0;
+    for (int k = rowptr[r]; k < rowptr[r + 1]; k++)
+      if (colidx[k] == r) d = vals[k];
+    dinv[r] = (pc == 1) ? ((d != 0.0) ? 1.0 / d : 1.0) : 1.0;
+  }
+  double *binv = NULL;
+  if (pc == 2) {
+    binv = calloc((size_t)g_nblk * 16, sizeof(double));
+    for (int k = 0; k < g_nblk; k++) {
+      int r0 = g_blk_ptr[k], bs = g_blk_ptr[k + 1] - r0;
+      double *B = binv + (size_t)k * 16;
+      for (int i = 0; i < bs; i++)
+        for (int p = rowptr[r0 + i]; p < rowptr[r0 + i + 1]; p++) {
+          int c = colidx[p];
+          if (c >= r0 && c < r0 + bs) B[i * bs + (c - r0)] = vals[p];
+        }
+      small_inverse(bs, B);
+    }
+  }
+  double *R = malloc(sizeof(double) * n), *RP = malloc(sizeof(double) * n), *V = calloc(n, sizeof(double));
+  double *T = malloc(sizeof(double) * n), *S = malloc(sizeof(double) * n), *P = calloc(n, sizeof(double));
+  conv_ctx cv = {0, 0, rtol, atol, dtol};
+  memset(x, 0, sizeof(double) * n);
+  /* r = M^-1 b (x0 = 0) */
+  pc_apply(n, pc, dinv, binv, b, R);
+  double dp = sqrt(vdot(n, R, R));
+  int its = 0;
+  int reason = converged(&cv, 0, dp);
+  if (reason == R_ITERATING) {
+    memcpy(RP, R, sizeof(double) * n);
+    double rhoold = 1.0, alpha = 1.0, omegaold = 1.0;
+    int i = 0;
+    do {
+      const double rho = vdot(n, R, RP);
+      const double beta = (rho / rhoold) * (alpha / omegaold);
+#pragma omp parallel for schedule(static)
+      for (int k = 0; k < n; k++) P[k] = 1.0 * R[k] + (-omegaold * beta) * V[k] + beta * P[k];
+      spmv(n, rowptr, colidx, vals, P, T);
+      pc_apply(n, pc, dinv, binv, T, V);
+      double d1 = vdot(n, V, RP);
+      if (d1 != d1 || isinf(d1)) { reason = R_DIV_NANORINF; break; }
+      if (d1 == 0.0) { reason = R_DIV_BREAKDOWN; break; }
+      alpha = rho / d1;
+#pragma omp parallel for schedule(static)
+      for (int k = 0; k < n; k++) S[k] = -alpha * V[k] + R[k];
+      spmv(n, rowptr, colidx, vals, S, R);
+      pc_apply(n, pc, dinv, binv, R, T);
+      d1 = vdot(n, S, T);
+      const double d2 = vdot(n, T, T);
+      if (d2 == 0.0) {
+        if (vdot(n, S, S) != 0.0) { reason = R_DIV_BREAKDOWN; break; }
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < n; k++) x[k] += alpha * P[k];
+        its++;
+        dp = 0.0;
+        reason = R_RTOL;
+        break;
+      }
+      const double omega = d1 / d2;
+#pragma omp parallel for schedule(static)
+      for (int k = 0; k < n; k++) {
+        x[k] = alpha * P[k] + omega * S[k] + 1.0 * x[k];
+        R[k] = -omega * T[k] + S[k];
+      }
+      dp = sqrt(vdot(n, R, R));
+      rhoold = rho;
+      omegaold = omega;
+      its++;
+      reason = converged(&cv, its, dp);
+      if (reason != R_ITERATING) break;
+      if (rho == 0.0) { reason = R_DIV_BREAKDOWN; break; }
+      i++;
+    } while (i < maxit);
+    if (reason == R_ITERATING) reason = R_DIV_ITS;
+  }
+  if (its_out) *its_out = its;
+  if (rnorm_out) *rnorm_out = dp;
+  free(dinv); free(binv); free(R); free(RP); free(V); free(T); free(S); free(P);
   return reason;
 }
 

@@ -15,8 +15,10 @@ Restates, file:line within the reference project:
   * SetTimeParametersFluid (src/base/UtilitiesGeneral.cpp:5-205)
 
 Linear solvers: ``lu`` (scipy SuperLU; stands in for the tests' MUMPS LU,
-testdata/*/petsc_options.dat) and ``gmres`` (oracle.c's restatement of PETSc
-3.10 GMRES with the jacobi PC).
+testdata/*/petsc_options.dat), ``gmres``, ``bcgs`` and ``preonly`` (oracle.c's
+restatements of PETSc 3.10 KSPGMRES, KSPBCGS and KSPPREONLY) with the jacobi,
+point-block jacobi or block-Jacobi ILU(k) preconditioner
+(input/petsc_options_gmres.dat, input/petsc_options_bcgs.dat).
 """
 from __future__ import annotations
 
@@ -68,6 +70,22 @@ def lib():
         L.orc_gmres.restype = ctypes.c_int
         L.orc_set_blocks.argtypes = [ctypes.c_int, _i32p]
         L.orc_set_blocks.restype = None
+        L.orc_bcgs.argtypes = [ctypes.c_int, _i32p, _i32p, _f64p, ctypes.c_int, _f64p, _f64p,
+                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+        L.orc_bcgs.restype = ctypes.c_int
+        L.orc_ilu_symbolic.argtypes = [ctypes.c_int, _i32p, _i32p, ctypes.c_int, _i32p, ctypes.c_int]
+        L.orc_ilu_symbolic.restype = ctypes.c_long
+        L.orc_ilu_numeric.argtypes = [_i32p, _i32p, _f64p, ctypes.c_int]
+        L.orc_ilu_numeric.restype = ctypes.c_int
+        L.orc_ilu_zero_pivot_row.argtypes = []
+        L.orc_ilu_zero_pivot_row.restype = ctypes.c_int
+        L.orc_ilu_apply.argtypes = [_f64p, _f64p, ctypes.c_int]
+        L.orc_ilu_apply.restype = None
+        L.orc_ilu_pattern.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_ilu_pattern.restype = None
+        L.orc_ilu_values.argtypes = [_f64p]
+        L.orc_ilu_values.restype = None
         L.orc_color.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p, _i32p]
         L.orc_color.restype = ctypes.c_int
         L.orc_norm2.argtypes = [ctypes.c_int, _f64p]
@@ -133,6 +151,20 @@ def time_params(tis: int, rho: float, dt: float) -> np.ndarray:
     return td
 
 
+def bjacobi_rows(nNode: int, ndof: int, dofmap: np.ndarray, nblocks: int) -> np.ndarray:
+    """Free-dof row offsets of the block-Jacobi blocks: nblocks contiguous node
+    ranges (nNode // nblocks nodes each, the first nNode % nblocks ranges one
+    more), each block starting at the first free row of its first node (the
+    free numbering is node-major).  The CUDA library cuts its blocks by the
+    same rule."""
+    nb = max(1, min(int(nblocks), nNode))
+    q, r = divmod(nNode, nb)
+    node_start = np.array([b * q + min(b, r) for b in range(nb + 1)], dtype=np.int64)
+    free = (dofmap.reshape(nNode, ndof) >= 0).sum(axis=1)
+    first_row = np.r_[0, np.cumsum(free)]
+    return np.ascontiguousarray(first_row[node_start].astype(np.int32))
+
+
 class OracleFEM:
     """CPU restatement of StabFEM's serial hot path.
 
@@ -144,13 +176,15 @@ class OracleFEM:
     def __init__(self, mesh, ctrl, solver: str = "gmres", restart: int = 50, rtol: float = 1e-10,
                  atol: float = 1e-50, dtol: float = 1e4, max_it: int = 10000, pc: str = "jacobi",
                  threads: int = 1, newton_tol: float = 1e-8, newton_max: int = 10, verbose: bool = False,
-                 form: str = "semi_implicit"):
+                 form: str = "semi_implicit", ilu_levels: int = 0, bjacobi_blocks: int = 1):
         self.mesh = mesh
         self.form = FORMULATIONS[form]
         self.ctrl = ctrl
         self.solver = solver
         self.restart, self.rtol, self.atol, self.dtol, self.max_it = restart, rtol, atol, dtol, max_it
-        self.pc = {"none": 0, "jacobi": 1, "pbjacobi": 2}[pc]
+        self.pc = {"none": 0, "jacobi": 1, "pbjacobi": 2, "bjacobi": 3}[pc]
+        self.ilu_levels, self.bjacobi_blocks = ilu_levels, bjacobi_blocks
+        self._ilu_ready = False
         self.threads = threads
         self.newton_tol, self.newton_max = newton_tol, newton_max
         self.verbose = verbose
@@ -176,6 +210,8 @@ class OracleFEM:
         owner = free // self.ndof
         starts = np.nonzero(np.r_[True, owner[1:] != owner[:-1]])[0] if len(free) else np.zeros(0, np.int64)
         self.blk_ptr = np.ascontiguousarray(np.r_[starts, len(free)].astype(np.int32))
+        # block-Jacobi blocks: contiguous node ranges cut at free-row offsets
+        self.bj_rows = bjacobi_rows(nN, self.ndof, self.dofmap, bjacobi_blocks)
         L = lib()
         self.rowptr = np.zeros(self.ntot + 1, dtype=np.int32)
         nnz = L.orc_pattern(nN, self.ndof, mesh.nElem, self.npe, self.conn, self.dofmap, self.ntot,
@@ -235,6 +271,16 @@ class OracleFEM:
         import scipy.sparse as sp
         return sp.csr_matrix((self.vals, self.colidx, self.rowptr), shape=(self.ntot, self.ntot))
 
+    def factor_ilu(self):
+        """Block-Jacobi ILU(k) factors of the current matrix (symbolic once)."""
+        L = lib()
+        if not self._ilu_ready:
+            L.orc_ilu_symbolic(self.ntot, self.rowptr, self.colidx, len(self.bj_rows) - 1, self.bj_rows,
+                               self.ilu_levels)
+            self._ilu_ready = True
+        if L.orc_ilu_numeric(self.rowptr, self.colidx, self.vals, self.threads) != 0:
+            raise RuntimeError(f"zero pivot in ILU at row {L.orc_ilu_zero_pivot_row()}")
+
     def linear_solve(self):
         if self.solver == "lu":
             import scipy.sparse.linalg as spla
@@ -243,11 +289,24 @@ class OracleFEM:
         x = np.zeros(self.ntot)
         if self.pc == 2:
             lib().orc_set_blocks(len(self.blk_ptr) - 1, self.blk_ptr)
+        if self.pc == 3:
+            self.factor_ilu()
         its = ctypes.c_int(0)
         rn = ctypes.c_double(0.0)
-        reason = lib().orc_gmres(self.ntot, self.rowptr, self.colidx, self.vals, self.pc, self.rhs, x,
-                                 self.restart, self.rtol, self.atol, self.dtol, self.max_it, ctypes.byref(its),
-                                 ctypes.byref(rn), self.threads)
+        if self.solver == "preonly":
+            # KSPSolve_PREONLY: one preconditioner application
+            if self.pc != 3:
+                raise ValueError("preonly is used with the bjacobi ILU/LU preconditioner")
+            lib().orc_ilu_apply(np.ascontiguousarray(self.rhs), x, self.threads)
+            return x, {"its": 1, "reason": 4, "rnorm": 0.0}
+        if self.solver == "bcgs":
+            reason = lib().orc_bcgs(self.ntot, self.rowptr, self.colidx, self.vals, self.pc, self.rhs, x,
+                                    self.rtol, self.atol, self.dtol, self.max_it, ctypes.byref(its),
+                                    ctypes.byref(rn), self.threads)
+        else:
+            reason = lib().orc_gmres(self.ntot, self.rowptr, self.colidx, self.vals, self.pc, self.rhs, x,
+                                     self.restart, self.rtol, self.atol, self.dtol, self.max_it,
+                                     ctypes.byref(its), ctypes.byref(rn), self.threads)
         return x, {"its": its.value, "reason": reason, "rnorm": rn.value}
 
     def step(self) -> Dict:
