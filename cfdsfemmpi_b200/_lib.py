@@ -21,6 +21,7 @@ EXPORTS = [
     "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
     "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
     "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual", "cfdgpu_residual_norm_noalloc",
+    "cfdgpu_ilu_export", "cfdgpu_pc_apply_export",
     "cfdgpu_mpnn_create", "cfdgpu_mpnn_destroy", "cfdgpu_mpnn_num_params", "cfdgpu_mpnn_get_params",
     "cfdgpu_mpnn_set_params", "cfdgpu_mpnn_set_scales", "cfdgpu_mpnn_add_sample", "cfdgpu_mpnn_num_samples",
     "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess_mode", "cfdgpu_set_guess",
@@ -29,10 +30,11 @@ EXPORTS = [
 ]
 GUESS = {"network": 1, "network_velocity": 2, "extrapolation": 4}
 FORM = {"semi_implicit": 0, "fully_implicit": 1}
-KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3}
+KIND = {"spmv": 0, "elem_k": 1, "elem_f": 2, "ortho": 3, "trsv": 4, "ilu": 5, "bcgs": 6}
 
 OK, EINVAL, ECUDA, ENEGJAC, EKSP, ENOMEM, ENODEV, ETOOBIG = 0, -1, -2, -3, -4, -5, -6, -7
-PC = {"none": 0, "jacobi": 1, "pbjacobi": 2}
+PC = {"none": 0, "jacobi": 1, "pbjacobi": 2, "bjacobi": 3}
+KSP = {"gmres": 0, "bcgs": 1, "preonly": 2}
 PREC = {"fp64": 0, "mixed": 1}
 MAX_NEWTON = 32
 
@@ -54,7 +56,8 @@ class SolverOpts(ctypes.Structure):
                 ("dtol", ctypes.c_double), ("max_it", ctypes.c_int), ("pc_type", ctypes.c_int),
                 ("precision", ctypes.c_int), ("inner_restart", ctypes.c_int), ("inner_rtol", ctypes.c_double),
                 ("reuse_tangent", ctypes.c_int), ("refine_rtol", ctypes.c_double), ("newton_rtol", ctypes.c_double),
-                ("formulation", ctypes.c_int)]
+                ("formulation", ctypes.c_int), ("ksp_type", ctypes.c_int), ("ilu_levels", ctypes.c_int),
+                ("bjacobi_blocks", ctypes.c_int), ("ilu_chunk", ctypes.c_int)]
 
 
 class StepStats(ctypes.Structure):
@@ -117,6 +120,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_solve_export.argtypes = [vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.cfdgpu_timers.argtypes = [vp, vp]
     L.cfdgpu_true_residual.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
+    L.cfdgpu_ilu_export.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), vp, vp, vp, vp, vp]
+    L.cfdgpu_pc_apply_export.argtypes = [vp, vp, vp]
     L.cfdgpu_residual_norm_noalloc.argtypes = [ip, ip, vp, vp, vp, vp, vp, vp, vp]
     L.cfdgpu_mpnn_create.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(vp)]
     L.cfdgpu_mpnn_destroy.argtypes = [vp]
@@ -182,12 +187,14 @@ def _mesh_struct(mesh):
 
 def _control_opts(ctrl, restart=50, rtol=1e-10, atol=1e-50, dtol=1e4, max_it=10000, pc="jacobi", precision="fp64",
                   inner_restart=0, inner_rtol=1e-4, reuse_tangent=True, newton_tol=1e-8, newton_max_iter=10,
-                  refine_rtol=1e-10, newton_rtol=0.0, formulation="semi_implicit"):
+                  refine_rtol=1e-10, newton_rtol=0.0, formulation="semi_implicit", ksp="gmres", ilu_levels=0,
+                  bjacobi_blocks=1, ilu_chunk=0):
     """(Control, SolverOpts) structs from an io.Control and solver keywords."""
     c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
                 ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
     o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
-                   1 if reuse_tangent else 0, refine_rtol, newton_rtol, FORM[formulation])
+                   1 if reuse_tangent else 0, refine_rtol, newton_rtol, FORM[formulation], KSP[ksp], ilu_levels,
+                   bjacobi_blocks, ilu_chunk)
     return c, o
 
 
@@ -222,7 +229,8 @@ class Handle:
                  max_it: int = 10000, pc: str = "jacobi", precision: str = "fp64", inner_restart: int = 0,
                  inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
                  newton_max_iter: int = 10, refine_rtol: float = 1e-10, newton_rtol: float = 0.0,
-                 guess: str = "constant", formulation: str = "semi_implicit"):
+                 guess: str = "constant", formulation: str = "semi_implicit", ksp: str = "gmres",
+                 ilu_levels: int = 0, bjacobi_blocks: int = 1, ilu_chunk: int = 0):
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()
@@ -232,7 +240,8 @@ class Handle:
         c, o = _control_opts(ctrl, restart=restart, rtol=rtol, atol=atol, dtol=dtol, max_it=max_it, pc=pc,
                              precision=precision, inner_restart=inner_restart, inner_rtol=inner_rtol,
                              reuse_tangent=reuse_tangent, newton_tol=newton_tol, newton_max_iter=newton_max_iter,
-                             refine_rtol=refine_rtol, newton_rtol=newton_rtol, formulation=formulation)
+                             refine_rtol=refine_rtol, newton_rtol=newton_rtol, formulation=formulation, ksp=ksp,
+                             ilu_levels=ilu_levels, bjacobi_blocks=bjacobi_blocks, ilu_chunk=ilu_chunk)
         rc = L.cfdgpu_create(ctypes.byref(m), ctypes.byref(c), ctypes.byref(o), ctypes.byref(self.h))
         if rc != 0:
             msg = L.cfdgpu_last_error(self.h).decode() if self.h else "create failed"
@@ -366,6 +375,31 @@ class Handle:
         its, reason = ctypes.c_int(), ctypes.c_int()
         self._check(self._L.cfdgpu_solve_export(self.h, _ptr(bb), _ptr(x), ctypes.byref(its), ctypes.byref(reason)))
         return x, its.value, reason.value
+
+    def ilu_factors(self, values: bool = True) -> dict:
+        """Block ILU factors of the last assembled matrix (pc='bjacobi'):
+        rowptr, colidx, diag and, with values=True, the L/U blocks (nnzb x
+        ndof x ndof) and the inverted diagonal blocks (nNode x ndof x ndof)."""
+        nnzb = ctypes.c_int64()
+        self._check(self._L.cfdgpu_ilu_export(self.h, ctypes.byref(nnzb), None, None, None, None, None))
+        nb = self.ndof
+        d = {"rowptr": np.zeros(self.nNode + 1, np.int32), "colidx": np.zeros(nnzb.value, np.int32),
+             "diag": np.zeros(self.nNode, np.int32)}
+        vals = np.zeros(nnzb.value * nb * nb) if values else None
+        dinv = np.zeros(self.nNode * nb * nb) if values else None
+        self._check(self._L.cfdgpu_ilu_export(self.h, None, _ptr(d["rowptr"]), _ptr(d["colidx"]), _ptr(d["diag"]),
+                                              _ptr(vals), _ptr(dinv)))
+        if values:
+            d["vals"] = vals.reshape(-1, nb, nb)
+            d["dinv"] = dinv.reshape(-1, nb, nb)
+        return d
+
+    def pc_apply(self, r: np.ndarray) -> np.ndarray:
+        """z = M^-1 r with the preconditioner of the last assembled matrix."""
+        rr = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros(self.n)
+        self._check(self._L.cfdgpu_pc_apply_export(self.h, _ptr(rr), _ptr(z)))
+        return z
 
     def true_residual(self, x: np.ndarray, b: np.ndarray) -> float:
         xx = np.ascontiguousarray(x, dtype=np.float64)

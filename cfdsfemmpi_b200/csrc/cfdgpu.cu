@@ -9,6 +9,7 @@
 //     blocks, FP64; FP32 copy in mixed mode), diag_slot per node
 //   element->block slot map nElem*npe*npe int32, colour-ordered element list
 //   Krylov basis (m+1) vectors, Hessenberg/Givens arrays, reduction scratch
+//   block ILU(k) factors (own BSR pattern), BiCGStab work vectors
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,7 +22,9 @@
 #include <vector>
 
 #include "../../include/cfdgpu.h"
+#include "bcgs_kernels.cuh"
 #include "element_kernels.cuh"
+#include "ilu_kernels.cuh"
 #include "internal.h"
 #include "linalg_kernels.cuh"
 #include "setup.h"
@@ -104,9 +107,21 @@ struct cfdgpu_handle {
   std::vector<int> pkind;                // kind of each recorded pair
   std::vector<double> pbytes;            // algorithmic bytes of each recorded launch
   int pused = 0;
-  int64_t prof_launches[CFDGPU_KIND_COUNT] = {0, 0, 0, 0};
-  double prof_ms[CFDGPU_KIND_COUNT] = {0, 0, 0, 0};
-  double prof_bytes[CFDGPU_KIND_COUNT] = {0, 0, 0, 0};
+  int64_t prof_launches[CFDGPU_KIND_COUNT] = {};
+  double prof_ms[CFDGPU_KIND_COUNT] = {};
+  double prof_bytes[CFDGPU_KIND_COUNT] = {};
+  // block-Jacobi ILU(k) preconditioner (pc_type CFDGPU_PC_BJACOBI_ILU)
+  IluPattern ilu;
+  int32_t *frow = nullptr, *fcol = nullptr, *fdiag = nullptr, *faslot = nullptr;
+  double *fval = nullptr, *fdinv = nullptr;
+  unsigned int *iflags = nullptr;
+  TriCtl *tctl = nullptr, *h_tctl = nullptr;
+  double *ptmp = nullptr;          // A x before the triangular solves
+  int ilu_chunk = 8;
+  // BiCGStab (ksp_type CFDGPU_KSP_BCGS)
+  BcgsState *bst = nullptr, *h_bst = nullptr;
+  double *bR = nullptr, *bRP = nullptr, *bP = nullptr, *bV = nullptr, *bS = nullptr, *bT = nullptr;
+  std::vector<cudaGraphExec_t> graphs_bcgs;
 };
 
 static const int PROF_POOL = 32768;
@@ -423,10 +438,95 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
   return 0;
 }
 
+// Persistent grid of the sync-free ILU kernels: enough warps for `tasks`
+// tasks, at most 4 CTAs of 8 warps per SM.
+static inline int ilu_grid(int64_t tasks)
+{
+  const int64_t ctas = (tasks + ILU_WARPS - 1) / ILU_WARPS;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(ctas, 148 * 4));
+}
+
+static double ilu_factor_bytes(cfdgpu_handle *h)
+{
+  // read A once, write the factors and the inverted diagonals once
+  const double bb = (double)h->ndof * h->ndof * 8.0;
+  return (double)h->topo.nnzb() * bb + (double)h->ilu.nnzb() * bb + (double)h->nNode * bb;
+}
+
+static double trsv_bytes(cfdgpu_handle *h)
+{
+  // both factors once (blocks + column indices), the inverted diagonals, and
+  // the vector in, intermediate (written and read) and out
+  const double bb = (double)h->ndof * h->ndof * 8.0, V = 8.0 * h->n;
+  return (double)h->ilu.nnzb() * (bb + 4.0) + (double)h->nNode * bb + 4.0 * V;
+}
+
+// numeric block ILU of the assembled FP64 matrix
+static int ilu_factor_run(cfdgpu_handle *h)
+{
+  const int pi = prof_begin(h, CFDGPU_KIND_ILU, ilu_factor_bytes(h));
+  const int grid = ilu_grid(h->nNode);
+  if (h->ndof == 4)
+    ilu_factor<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
+                                                                      h->fcol, h->fdiag, h->fval, h->fdinv, h->iflags,
+                                                                      h->tctl);
+  else
+    ilu_factor<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
+                                                                      h->fcol, h->fdiag, h->fval, h->fdinv, h->iflags,
+                                                                      h->tctl);
+  prof_end(h, pi);
+  LAUNCHED(h);
+  return check_launch(h, "ilu_factor");
+}
+
+// z = (L U)^-1 r: lower solve r -> z, upper solve in place on z
+static int ilu_apply(cfdgpu_handle *h, const double *r, double *z, const GmresState *st, int j, const int *active)
+{
+  const int pi = prof_begin(h, CFDGPU_KIND_TRSV, trsv_bytes(h));
+  const int chunk = h->ilu_chunk;
+  const int grid = ilu_grid((h->nNode + chunk - 1) / chunk);
+  if (h->ndof == 4) {
+    ilu_lsolve<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
+                                                                      h->fval, r, z, h->iflags, h->tctl, st, j, active);
+    ilu_usolve<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
+                                                                      h->fval, h->fdinv, z, z, h->iflags, h->tctl, st,
+                                                                      j, active);
+  } else {
+    ilu_lsolve<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
+                                                                      h->fval, r, z, h->iflags, h->tctl, st, j, active);
+    ilu_usolve<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
+                                                                      h->fval, h->fdinv, z, z, h->iflags, h->tctl, st,
+                                                                      j, active);
+  }
+  prof_end(h, pi);
+  h->launches += 2;
+  return check_launch(h, "ilu_solve");
+}
+
+// errors recorded by the ILU kernels since the last check (zero pivot in the
+// factorisation, a dependency wait that ran out); clears them
+static int ilu_check(cfdgpu_handle *h)
+{
+  if (!h->tctl) return 0;
+  CK(cudaMemcpyAsync(h->h_tctl, h->tctl, sizeof(TriCtl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const TriCtl c = *h->h_tctl;
+  if (c.error == 0) return 0;
+  CK(cudaMemsetAsync(&h->tctl->error, 0, sizeof(unsigned int), h->stream));
+  if (c.error == ILU_ERR_ZERO_PIVOT) {
+    h->err = "Zero pivot in the ILU factorisation (singular diagonal block at node " +
+             std::to_string(c.zero_pivot_row) + ")";
+    return CFDGPU_EKSP;
+  }
+  h->err = "ILU triangular solve: a dependency wait timed out";
+  return CFDGPU_ECUDA;
+}
+
 static int build_pc(cfdgpu_handle *h)
 {
   const int pc = h->opts.pc_type;
   if (pc == CFDGPU_PC_NONE) return 0;
+  if (pc == CFDGPU_PC_BJACOBI_ILU) return ilu_factor_run(h);
   const int g = (h->nNode + 127) / 128;
   if (h->mixed && h->ndof == 4) {
     build_jacobi<4, float, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr32, h->dinv32, h->binv32, pc);
@@ -452,15 +552,23 @@ static double spmv_bytes(cfdgpu_handle *h, int mode, int vbytes, int mbytes, int
 
 // y = M^-1 (A x) (mode 0) or y = M^-1 (b - A x) (mode 1), FP64 vectors
 static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y, const GmresState *st, int j,
-                   const double *xscale = nullptr)
+                   const double *xscale = nullptr, const int *active = nullptr)
 {
   const int pc = h->opts.pc_type;
+  if (pc == CFDGPU_PC_BJACOBI_ILU) {
+    // y = (LU)^-1 (A x) or (LU)^-1 (b - A x): SpMV into the scratch vector, then the two solves
+    h->opts.pc_type = CFDGPU_PC_NONE;
+    int rc = spmv_pc(h, mode, x, b, h->ptmp, st, j, xscale, active);
+    h->opts.pc_type = CFDGPU_PC_BJACOBI_ILU;
+    if (rc) return rc;
+    return ilu_apply(h, h->ptmp, y, st, j, active);
+  }
   const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, mode, 8, 8, pc));
   if (h->ndof == 4) {
     const int grid = (int)((h->nNode * 32LL + 255) / 256);
 #define SPMV4(MO, PCV)                                                                                          \
   bsr4_spmv<MO, PCV, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, h->dinv, \
-                                                           h->binv, y, st, j, xscale)
+                                                           h->binv, y, st, j, xscale, active)
     if (mode == 0) {
       if (pc == 0) SPMV4(0, 0); else if (pc == 1) SPMV4(0, 1); else SPMV4(0, 2);
     } else {
@@ -471,7 +579,7 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
     const int grid = (int)((h->n + 255) / 256);
 #define SPMV3(MO, PCV)                                                                                        \
   bsr_spmv_generic<3, MO, PCV, double><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr, x, b, \
-                                                                     h->dinv, h->binv, y, st, j, xscale)
+                                                                     h->dinv, h->binv, y, st, j, xscale, active)
     if (mode == 0) {
       if (pc == 0) SPMV3(0, 0); else if (pc == 1) SPMV3(0, 1); else SPMV3(0, 2);
     } else {
@@ -656,14 +764,23 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
 }
 
 // Restarted GMRES on the assembled FP64 BSR: x = A^-1 b, x0 = 0.
-static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+// z = M^-1 r with the handle's FP64 preconditioner
+static int pc_apply_vec(cfdgpu_handle *h, const double *r, double *z, const int *active = nullptr)
 {
   const int64_t n = h->n;
+  if (h->opts.pc_type == CFDGPU_PC_BJACOBI_ILU) return ilu_apply(h, r, z, nullptr, 0, active);
   if (h->ndof == 4)
-    pc_apply<4, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, h->V);
+    pc_apply<4, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, r, z);
   else
-    pc_apply<3, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, b, h->V);
+    pc_apply<3, double, double><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv, h->binv, r, z);
   LAUNCHED(h);
+  return check_launch(h, "pc_apply");
+}
+
+static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+{
+  int rc0 = pc_apply_vec(h, b, h->V);
+  if (rc0) return rc0;
   Krylov<double> K(h->graphs64);
   K.V = h->V; K.m = h->m; K.ldv = h->ldv; K.st = h->gst; K.ga = h->ga;
   auto arn = [&](int j) {
@@ -672,6 +789,114 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
   auto res = [&]() { return spmv_pc(h, 1, x, b, h->V, nullptr, 0, nullptr); };
   return gmres_run<double>(h, K, x, h->opts.max_it, h->opts.rtol, h->opts.atol, h->opts.dtol, false, arn, res,
                            its_out, reason_out);
+}
+
+// BiCGStab (PETSc KSPBCGS semantics, left preconditioning, x0 = 0) on the
+// assembled FP64 BSR: x = A^-1 b.  Iterations are enqueued in chunks of
+// h->chunk / 2 (captured once as a CUDA graph and replayed: every iteration
+// runs the same kernels on the same buffers), and the host polls the device
+// control block `depth` chunks behind; iterations after the solve has ended
+// return at once.
+static int bcgs(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+{
+  const int64_t n = h->n;
+  int rc;
+  BcgsState *st = h->bst;
+  const int *act = &st->active;
+  bcgs_setup<<<1, 1, 0, h->stream>>>(st, h->opts.max_it, h->opts.rtol, h->opts.atol, h->opts.dtol);
+  LAUNCHED(h);
+  CK(cudaMemsetAsync(x, 0, sizeof(double) * n, h->stream));
+  if ((rc = pc_apply_vec(h, b, h->bR))) return rc;
+  bcgs_init<double><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, h->bR, h->bRP, h->bP, h->bV, st, h->red_partial2);
+  LAUNCHED(h);
+  if ((rc = check_launch(h, "bcgs_init"))) return rc;
+  const int vgrid = grid_for(n);
+  const double V = 8.0 * n;
+  auto iteration = [&]() -> int {
+    int r;
+    int pi = prof_begin(h, CFDGPU_KIND_BCGS, 4.0 * V);
+    bcgs_p<double><<<vgrid, 256, 0, h->stream>>>(n, h->bR, h->bV, h->bP, st);
+    prof_end(h, pi);
+    if ((r = spmv_pc(h, 0, h->bP, nullptr, h->bV, nullptr, 0, nullptr, act))) return r;
+    pi = prof_begin(h, CFDGPU_KIND_BCGS, 5.0 * V);
+    bcgs_alpha<double><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, h->bV, h->bRP, st, h->red_partial2);
+    bcgs_s<double><<<vgrid, 256, 0, h->stream>>>(n, h->bR, h->bV, h->bS, st);
+    prof_end(h, pi);
+    if ((r = spmv_pc(h, 0, h->bS, nullptr, h->bT, nullptr, 0, nullptr, act))) return r;
+    pi = prof_begin(h, CFDGPU_KIND_BCGS, 10.0 * V);
+    bcgs_omega<double><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, h->bS, h->bT, st, h->red_partial2);
+    bcgs_xr<double><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, x, h->bP, h->bS, h->bT, h->bR, h->bRP, st,
+                                                              h->red_partial2);
+    prof_end(h, pi);
+    h->launches += 5;
+    return check_launch(h, "bcgs_iteration");
+  };
+  const int CH = std::max(1, h->chunk / 2);
+  const int D = h->depth, R = D + 1;
+  const int64_t max_chunks = (int64_t)h->opts.max_it / CH + D + 2;
+  bool stop = false;
+  for (int64_t c = 0; c < max_chunks && !stop; c++) {
+    if (h->use_graphs && !h->prof) {
+      if (h->graphs_bcgs.empty()) h->graphs_bcgs.resize(1, nullptr);
+      cudaGraphExec_t &ex = h->graphs_bcgs[0];
+      if (!ex) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t before = h->launches;
+        int r = 0;
+        for (int k = 0; k < CH && !r; k++) r = iteration();
+        const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+        if (r) return r;
+        if (ec != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(ec); return CFDGPU_ECUDA; }
+        CK(cudaGraphInstantiate(&ex, g, 0));
+        CK(cudaGraphDestroy(g));
+        h->launches = before;
+      }
+      CK(cudaGraphLaunch(ex, h->stream));
+      const int per_it = (h->opts.pc_type == CFDGPU_PC_BJACOBI_ILU) ? 11 : 7;
+      h->launches += (int64_t)CH * per_it;
+    } else {
+      for (int k = 0; k < CH; k++)
+        if ((rc = iteration())) return rc;
+    }
+    const int cidx = (int)(c % R);
+    CK(cudaMemcpyAsync(&h->h_bst[cidx], st, sizeof(BcgsState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaEventRecord(h->evq[cidx], h->stream));
+    if (c >= D) {
+      const int pidx = (int)((c - D) % R);
+      CK(cudaEventSynchronize(h->evq[pidx]));
+      if (!h->h_bst[pidx].active) stop = true;
+    }
+  }
+  BcgsState *fin = h->h_bst + cfdgpu_handle::MAX_DEPTH + 1;
+  CK(cudaMemcpyAsync(fin, st, sizeof(BcgsState), cudaMemcpyDeviceToHost, h->stream));
+  if ((rc = host_wait(h))) return rc;
+  if ((rc = ilu_check(h))) return rc;
+  int reason = fin->reason;
+  if (reason == 0) reason = -3;   // the chunk cap ended the loop (maxit normally ends the solve first)
+  if (its_out) *its_out = fin->its;
+  if (reason_out) *reason_out = reason;
+  return 0;
+}
+
+// Linear solve of the FP64 system with the handle's Krylov method
+static int krylov_solve(cfdgpu_handle *h, const double *b, double *x, int *its, int *reason)
+{
+  int rc;
+  if (h->opts.ksp_type == CFDGPU_KSP_BCGS) {
+    rc = bcgs(h, b, x, its, reason);
+  } else if (h->opts.ksp_type == CFDGPU_KSP_PREONLY) {
+    // KSPSolve_PREONLY: one application of the preconditioner
+    rc = pc_apply_vec(h, b, x);
+    if (!rc) rc = host_wait(h);
+    if (!rc) rc = ilu_check(h);
+    if (its) *its = 1;
+    if (reason) *reason = 4;   // KSP_CONVERGED_ITS
+  } else {
+    rc = gmres(h, b, x, its, reason);
+    if (!rc) rc = ilu_check(h);
+  }
+  return rc;
 }
 
 // Mixed precision linear solve (4x4 blocks): FP64 iterative refinement around
@@ -797,6 +1022,7 @@ int set_host_schedule(cfdgpu_handle *h, bool blocking, int chunk, int depth)
     CK(cudaStreamSynchronize(h->stream));
     for (auto &g : h->graphs64) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     for (auto &g : h->graphs32) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &g : h->graphs_bcgs) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     h->chunk = chunk;
   }
   return 0;
@@ -861,6 +1087,30 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   if (h->opts.max_it <= 0) h->opts.max_it = 10000;
   if (h->opts.formulation != CFDGPU_FORM_SEMI_IMPLICIT && h->opts.formulation != CFDGPU_FORM_FULLY_IMPLICIT) {
     h->err = "unknown element formulation";
+    return CFDGPU_EINVAL;
+  }
+  if (h->opts.ksp_type != CFDGPU_KSP_GMRES && h->opts.ksp_type != CFDGPU_KSP_BCGS &&
+      h->opts.ksp_type != CFDGPU_KSP_PREONLY) {
+    h->err = "unknown Krylov method";
+    return CFDGPU_EINVAL;
+  }
+  if (h->opts.pc_type < CFDGPU_PC_NONE || h->opts.pc_type > CFDGPU_PC_BJACOBI_ILU) {
+    h->err = "unknown preconditioner";
+    return CFDGPU_EINVAL;
+  }
+  if (h->opts.pc_type == CFDGPU_PC_BJACOBI_ILU) {
+    if (h->opts.precision != CFDGPU_PREC_FP64) {
+      h->err = "the block ILU preconditioner runs in FP64 precision mode";
+      return CFDGPU_EINVAL;
+    }
+    if (h->opts.ilu_chunk < 0 || h->opts.ilu_chunk > ILU_MAX_CHUNK) {
+      h->err = "ilu_chunk must lie in [0, 32]";
+      return CFDGPU_EINVAL;
+    }
+    h->ilu_chunk = (h->opts.ilu_chunk > 0) ? h->opts.ilu_chunk : 8;
+  }
+  if (h->opts.ksp_type != CFDGPU_KSP_GMRES && h->opts.precision != CFDGPU_PREC_FP64) {
+    h->err = "BiCGStab and preonly run in FP64 precision mode";
     return CFDGPU_EINVAL;
   }
   if (h->ctrl.newton_max_iter <= 0) h->ctrl.newton_max_iter = 10;
@@ -970,6 +1220,37 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   CK(cudaMemset(h->gst, 0, sizeof(GmresState)));
   CK(cudaMallocHost(&h->h_scalar, 8 * sizeof(double)));
   CK(cudaMallocHost(&h->h_gst, (cfdgpu_handle::MAX_DEPTH + 2) * sizeof(GmresState)));
+  if (h->opts.pc_type == CFDGPU_PC_BJACOBI_ILU) {
+    const int nblk = (h->opts.bjacobi_blocks > 0) ? h->opts.bjacobi_blocks : 1;
+    std::string m2 = build_ilu_pattern(t, h->opts.ilu_levels, nblk, h->ilu);
+    if (!m2.empty()) { h->err = m2; return CFDGPU_EINVAL; }
+    const IluPattern &f = h->ilu;
+    if ((rc = upload(h, &h->frow, f.rowptr.data(), f.rowptr.size()))) return rc;
+    if ((rc = upload(h, &h->fcol, f.colidx.data(), f.colidx.size()))) return rc;
+    if ((rc = upload(h, &h->fdiag, f.diag.data(), f.diag.size()))) return rc;
+    if ((rc = upload(h, &h->faslot, f.aslot.data(), f.aslot.size()))) return rc;
+    if ((rc = dalloc(h, &h->fval, (size_t)f.nnzb() * bb))) return rc;
+    CK(cudaMemset(h->fval, 0, sizeof(double) * f.nnzb() * bb));
+    if ((rc = dalloc(h, &h->fdinv, (size_t)h->nNode * bb))) return rc;
+    CK(cudaMemset(h->fdinv, 0, sizeof(double) * h->nNode * bb));
+    if ((rc = dalloc(h, &h->iflags, (size_t)h->nNode))) return rc;
+    CK(cudaMemset(h->iflags, 0, sizeof(unsigned int) * h->nNode));
+    if ((rc = dalloc(h, &h->tctl, 1))) return rc;
+    CK(cudaMemset(h->tctl, 0, sizeof(TriCtl)));
+    if ((rc = dalloc(h, &h->ptmp, (size_t)n))) return rc;
+    CK(cudaMemset(h->ptmp, 0, sizeof(double) * n));
+    CK(cudaMallocHost(&h->h_tctl, sizeof(TriCtl)));
+  }
+  if (h->opts.ksp_type == CFDGPU_KSP_BCGS) {
+    double **bv[] = {&h->bR, &h->bRP, &h->bP, &h->bV, &h->bS, &h->bT};
+    for (double **v : bv) {
+      if ((rc = dalloc(h, v, (size_t)n))) return rc;
+      CK(cudaMemset(*v, 0, sizeof(double) * n));
+    }
+    if ((rc = dalloc(h, &h->bst, 1))) return rc;
+    CK(cudaMemset(h->bst, 0, sizeof(BcgsState)));
+    CK(cudaMallocHost(&h->h_bst, (cfdgpu_handle::MAX_DEPTH + 2) * sizeof(BcgsState)));
+  }
   CK(cudaDeviceSynchronize());
   h->timers[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return 0;
@@ -985,6 +1266,9 @@ int cfdgpu_destroy(cfdgpu_handle *h)
   for (auto &e : h->pev) cudaEventDestroy(e);
   for (auto g : h->graphs64) if (g) cudaGraphExecDestroy(g);
   for (auto g : h->graphs32) if (g) cudaGraphExecDestroy(g);
+  for (auto g : h->graphs_bcgs) if (g) cudaGraphExecDestroy(g);
+  if (h->h_tctl) cudaFreeHost(h->h_tctl);
+  if (h->h_bst) cudaFreeHost(h->h_bst);
   for (auto &e : h->evq)
     if (e) cudaEventDestroy(e);
   if (h->evw) cudaEventDestroy(h->evw);
@@ -1153,7 +1437,7 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     if (h->mixed) {
       if ((rc = solve_mixed(h, h->rhs, h->dx, &its, &passes, &reason))) return rc;
     } else {
-      if ((rc = gmres(h, h->rhs, h->dx, &its, &reason))) return rc;
+      if ((rc = krylov_solve(h, h->rhs, h->dx, &its, &reason))) return rc;
     }
     stats->ksp_its[iter] = its;
     stats->ksp_reason[iter] = reason;
@@ -1346,13 +1630,47 @@ int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, 
   int rc = build_pc(h);
   if (rc) return rc;
   int i = 0, r = 0;
-  rc = gmres(h, h->rhs, h->dx, &i, &r);
+  rc = krylov_solve(h, h->rhs, h->dx, &i, &r);
   if (rc) return rc;
   CK(cudaMemcpyAsync(x, h->dx, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (its) *its = i;
   if (reason) *reason = r;
   return 0;
+}
+
+int cfdgpu_ilu_export(cfdgpu_handle *h, int64_t *nnzb, int32_t *rowptr, int32_t *colidx, int32_t *diag, double *vals,
+                      double *dinv)
+{
+  if (!h) return CFDGPU_EINVAL;
+  if (h->opts.pc_type != CFDGPU_PC_BJACOBI_ILU) { h->err = "the handle has no ILU preconditioner"; return CFDGPU_EINVAL; }
+  const IluPattern &f = h->ilu;
+  if (nnzb) *nnzb = f.nnzb();
+  auto cp = [](int32_t *dst, const std::vector<int32_t> &v) { if (dst && !v.empty()) memcpy(dst, v.data(), v.size() * 4); };
+  cp(rowptr, f.rowptr); cp(colidx, f.colidx); cp(diag, f.diag);
+  if (!vals && !dinv) return 0;
+  if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
+  int rc = build_pc(h);
+  if (rc) return rc;
+  const size_t bb = (size_t)h->ndof * h->ndof;
+  if (vals) CK(cudaMemcpyAsync(vals, h->fval, sizeof(double) * f.nnzb() * bb, cudaMemcpyDeviceToHost, h->stream));
+  if (dinv) CK(cudaMemcpyAsync(dinv, h->fdinv, sizeof(double) * h->nNode * bb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return ilu_check(h);
+}
+
+int cfdgpu_pc_apply_export(cfdgpu_handle *h, const double *r, double *z)
+{
+  if (!h || !r || !z) return CFDGPU_EINVAL;
+  if (h->mixed) { h->err = "cfdgpu_pc_apply_export uses the FP64 preconditioner"; return CFDGPU_EINVAL; }
+  if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
+  int rc = build_pc(h);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->rhs, r, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = pc_apply_vec(h, h->rhs, h->dx))) return rc;
+  CK(cudaMemcpyAsync(z, h->dx, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return ilu_check(h);
 }
 
 int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm)

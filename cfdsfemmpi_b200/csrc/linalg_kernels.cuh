@@ -108,9 +108,11 @@ __global__ void __launch_bounds__(256)
 bsr4_spmv(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
               const MT *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
               const double *__restrict__ dinv, const double *__restrict__ binv, double *__restrict__ y,
-              const GmresState *__restrict__ st, int j, const double *__restrict__ xscale)
+              const GmresState *__restrict__ st, int j, const double *__restrict__ xscale,
+              const int *__restrict__ active = nullptr)
 {
   if (st && (!st->active || st->it != j)) return;
+  if (active && !active[0]) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nrows) return;
@@ -205,9 +207,10 @@ __global__ void bsr_spmv_generic(int nrows, const int32_t *__restrict__ rowptr, 
                                  const VT *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
                                  const double *__restrict__ dinv, const double *__restrict__ binv,
                                  double *__restrict__ y, const GmresState *__restrict__ st, int j,
-                                 const double *__restrict__ xscale)
+                                 const double *__restrict__ xscale, const int *__restrict__ active = nullptr)
 {
   if (st && (!st->active || st->it != j)) return;
+  if (active && !active[0]) return;
   const double xs = xscale ? xscale[0] : 1.0;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t node = t / NB;

@@ -2,6 +2,7 @@
 #include "setup.h"
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <numeric>
 
@@ -137,6 +138,89 @@ std::string build_topology(int nNode, int nElem, int npe, int ndof, const int32_
       t.dbc_mult.push_back(mult[g]);
     } else {
       t.dofmap[g] = t.nfree++;
+    }
+  }
+  return "";
+}
+
+std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPattern &f)
+{
+  f = IluPattern();
+  const int n = t.nNode;
+  if (levels < -1 || levels > 16) return "ILU levels must lie in [0, 16], or -1 for a complete factorisation";
+  const int nb = std::max(1, std::min(nblocks, n));
+  f.levels = levels;
+  f.nblocks = nb;
+  if (levels < 0) levels = 1 << 29;
+  f.blk.resize(nb + 1);
+  {
+    const int q = n / nb, r = n % nb;
+    for (int b = 0; b <= nb; b++) f.blk[b] = b * q + std::min(b, r);
+  }
+  const uint8_t all = (uint8_t)((1u << t.ndof) - 1u);
+  auto fixed_node = [&](int v) { return (t.fixmask[v] & all) == all; };
+  std::vector<int32_t> blk_of(n);
+  for (int b = 0; b < nb; b++)
+    for (int v = f.blk[b]; v < f.blk[b + 1]; v++) blk_of[v] = b;
+  // per-row sorted linked list over column nodes (n = end marker)
+  std::vector<int32_t> next(n + 1), lv(n);
+  std::vector<int32_t> ulev;       // level of every stored entry
+  f.rowptr.assign(n + 1, 0);
+  f.diag.assign(n, -1);
+  f.colidx.reserve(t.colidx.size());
+  ulev.reserve(t.colidx.size());
+  for (int i = 0; i < n; i++) {
+    int head = n, tail = -1;
+    auto push = [&](int c) {
+      lv[c] = 0;
+      if (tail < 0) head = c; else next[tail] = c;
+      tail = c;
+    };
+    if (fixed_node(i)) {
+      push(i);
+    } else {
+      for (int k = t.rowptr[i]; k < t.rowptr[i + 1]; k++) {
+        const int c = t.colidx[k];
+        if (blk_of[c] != blk_of[i] || (c != i && fixed_node(c))) continue;
+        push(c);
+      }
+    }
+    if (tail >= 0) next[tail] = n;
+    for (int p = head; p < i; p = next[p]) {
+      const int lp = lv[p];
+      if (lp + 1 > levels) continue;
+      int ins = p;
+      for (int q = f.diag[p] + 1; q < f.rowptr[p + 1]; q++) {
+        const int j = f.colidx[q];
+        const int l = lp + ulev[q] + 1;
+        if (l > levels) continue;
+        while (next[ins] < j) ins = next[ins];
+        if (next[ins] == j) {
+          if (l < lv[j]) lv[j] = l;
+        } else {
+          next[j] = next[ins];
+          next[ins] = j;
+          lv[j] = l;
+        }
+        ins = j;
+      }
+    }
+    for (int c = head; c < n; c = next[c]) {
+      if (c == i) f.diag[i] = (int32_t)f.colidx.size();
+      if ((int64_t)f.colidx.size() >= INT32_MAX) return "ILU factors exceed 2^31 blocks";
+      f.colidx.push_back(c);
+      ulev.push_back(lv[c]);
+    }
+    f.rowptr[i + 1] = (int32_t)f.colidx.size();
+    if (f.diag[i] < 0) return "node without a diagonal block";
+  }
+  // blocks of A inside the factor pattern
+  f.aslot.assign(t.colidx.size(), -1);
+  for (int i = 0; i < n; i++) {
+    const int32_t *b = f.colidx.data() + f.rowptr[i], *e = f.colidx.data() + f.rowptr[i + 1];
+    for (int k = t.rowptr[i]; k < t.rowptr[i + 1]; k++) {
+      const int32_t *p = std::lower_bound(b, e, t.colidx[k]);
+      if (p != e && *p == t.colidx[k]) f.aslot[k] = (int32_t)(p - f.colidx.data());
     }
   }
   return "";

@@ -41,6 +41,30 @@ struct Topology {
   int64_t nnzb() const { return (int64_t)colidx.size(); }
 };
 
+// Block ILU(k) structure of a block-Jacobi preconditioner on the BSR pattern
+// (PETSc PCBJACOBI with sub-PC ILU(levels), input/petsc_options_gmres.dat:2-5):
+// nodes are cut into nblocks contiguous ranges (nNode/nblocks nodes each, the
+// first nNode%nblocks ranges one longer), couplings between ranges are
+// dropped, and each range gets the level-of-fill pattern of ILU(levels) in
+// natural node order, lev(i,j) = min over pivots p of lev(i,p) + lev(p,j) + 1
+// with the blocks of A at level 0.  A node whose dofs are all prescribed has
+// an identity row and column in the BSR matrix and no row in the
+// reference's free-dof system: it keeps only its diagonal block and takes no
+// part in any other row, so the block factors equal the scalar ILU(levels)
+// of the free-dof matrix in exact arithmetic.  levels = -1 keeps all fill:
+// the complete LU of each range (one range: -pc_type lu).
+struct IluPattern {
+  int levels = 0, nblocks = 1;
+  std::vector<int32_t> rowptr;   // nNode+1
+  std::vector<int32_t> colidx;   // sorted per row
+  std::vector<int32_t> diag;     // position of the diagonal block of each row
+  std::vector<int32_t> aslot;    // per block of A: its position in the factors, or -1
+  std::vector<int32_t> blk;      // nblocks+1 node offsets
+  int64_t nnzb() const { return (int64_t)colidx.size(); }
+};
+
+std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPattern &f);
+
 // Returns "" on success, else an error message.
 std::string build_topology(int nNode, int nElem, int npe, int ndof, const int32_t *conn, int nDBC,
                            const int32_t *dbc_node, const int32_t *dbc_dof, const double *dbc_value,

@@ -123,14 +123,24 @@ void StabFEM::prepareInputData()
 
 std::string StabFEM::solverDescription() const
 {
-  const char *pc[] = {"none", "jacobi", "pbjacobi"};
+  const char *pc[] = {"none", "jacobi", "pbjacobi", "bjacobi"};
   std::ostringstream o;
-  o << "GMRES(" << opts_.restart << ") pc=" << pc[opts_.pc_type] << " rtol=" << opts_.rtol
-    << " max_it=" << opts_.max_it;
+  if (opts_.ksp_type == CFDGPU_KSP_BCGS) o << "BCGS";
+  else if (opts_.ksp_type == CFDGPU_KSP_PREONLY) o << "preonly";
+  else o << "GMRES(" << opts_.restart << ")";
+  o << " pc=" << pc[opts_.pc_type];
+  if (opts_.pc_type == CFDGPU_PC_BJACOBI_ILU) {
+    o << "[" << (opts_.bjacobi_blocks > 0 ? opts_.bjacobi_blocks : 1) << " x ";
+    if (opts_.ilu_levels < 0) o << "LU]";
+    else o << "ILU(" << opts_.ilu_levels << ")]";
+  }
+  o << " rtol=" << opts_.rtol << " max_it=" << opts_.max_it;
   return o.str();
 }
 
-// setSolver + prepareMatrixPattern (src/base/StabFEM2.cpp:10-319)
+// setSolver + prepareMatrixPattern (src/base/StabFEM2.cpp:10-319).  PETSc
+// option names with PETSc's defaults for a serial run; a method the library
+// does not implement is an error, never replaced by another one.
 int StabFEM::setSolver(int slv, int *parm, bool cIO)
 {
   (void)slv; (void)parm; (void)cIO;
@@ -138,21 +148,46 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
     auto it = options.find(k);
     return it == options.end() ? std::string(d) : it->second;
   };
-  const std::string ksp = get("-ksp_type", "gmres"), pc = get("-pc_type", "");
+  const std::string ksp = get("-ksp_type", "gmres"), pc = get("-pc_type", "ilu");
+  opts_ = cfdgpu_solver_opts{};
   opts_.restart = 30; opts_.rtol = 1e-5; opts_.atol = 1e-50; opts_.dtol = 1e4; opts_.max_it = 10000;
-  opts_.pc_type = CFDGPU_PC_PBJACOBI; opts_.precision = CFDGPU_PREC_FP64; opts_.inner_restart = 0;
+  opts_.precision = CFDGPU_PREC_FP64; opts_.inner_restart = 0;
   opts_.inner_rtol = 1e-4; opts_.reuse_tangent = 1; opts_.refine_rtol = 1e-10; opts_.newton_rtol = 0.0;
-  const bool direct = (ksp == "preonly" || pc == "lu" || pc == "cholesky");
-  if (direct) {
-    // no direct solver on the GPU: tight GMRES + point-block Jacobi substitutes
-    opts_.restart = 300; opts_.rtol = 1e-14; opts_.max_it = 50000;
-  } else {
-    if (pc == "jacobi") opts_.pc_type = CFDGPU_PC_JACOBI;
-    else if (pc == "none") opts_.pc_type = CFDGPU_PC_NONE;
-    if (options.count("-ksp_gmres_restart")) opts_.restart = std::atoi(options["-ksp_gmres_restart"].c_str());
-    if (options.count("-ksp_rtol")) opts_.rtol = std::atof(options["-ksp_rtol"].c_str());
-    if (options.count("-ksp_max_it")) opts_.max_it = std::atoi(options["-ksp_max_it"].c_str());
+  if (ksp == "gmres") opts_.ksp_type = CFDGPU_KSP_GMRES;
+  else if (ksp == "bcgs") opts_.ksp_type = CFDGPU_KSP_BCGS;
+  else if (ksp == "preonly") opts_.ksp_type = CFDGPU_KSP_PREONLY;
+  else {
+    std::cerr << " -ksp_type " << ksp << " is not implemented (gmres, bcgs, preonly)" << std::endl;
+    return CFDGPU_EINVAL;
   }
+  opts_.bjacobi_blocks = 1;
+  if (pc == "none") opts_.pc_type = CFDGPU_PC_NONE;
+  else if (pc == "jacobi") opts_.pc_type = CFDGPU_PC_JACOBI;
+  else if (pc == "pbjacobi") opts_.pc_type = CFDGPU_PC_PBJACOBI;
+  else if (pc == "ilu" || pc == "lu") {
+    opts_.pc_type = CFDGPU_PC_BJACOBI_ILU;
+    opts_.ilu_levels = (pc == "lu") ? -1 : std::atoi(get("-pc_factor_levels", "0").c_str());
+  } else if (pc == "bjacobi") {
+    const std::string sub = get("-sub_pc_type", "ilu");
+    if (sub != "ilu" && sub != "lu") {
+      std::cerr << " -sub_pc_type " << sub << " is not implemented (ilu, lu)" << std::endl;
+      return CFDGPU_EINVAL;
+    }
+    if (get("-sub_ksp_type", "preonly") != "preonly") {
+      std::cerr << " -sub_ksp_type must be preonly" << std::endl;
+      return CFDGPU_EINVAL;
+    }
+    opts_.pc_type = CFDGPU_PC_BJACOBI_ILU;
+    opts_.ilu_levels = (sub == "lu") ? -1 : std::atoi(get("-sub_pc_factor_levels", "0").c_str());
+    opts_.bjacobi_blocks = std::atoi(get("-pc_bjacobi_blocks", "1").c_str());
+  } else {
+    std::cerr << " -pc_type " << pc << " is not implemented (none, jacobi, pbjacobi, ilu, lu, bjacobi)" << std::endl;
+    return CFDGPU_EINVAL;
+  }
+  if (options.count("-ksp_gmres_restart")) opts_.restart = std::atoi(options["-ksp_gmres_restart"].c_str());
+  if (options.count("-ksp_rtol")) opts_.rtol = std::atof(options["-ksp_rtol"].c_str());
+  if (options.count("-ksp_max_it")) opts_.max_it = std::atoi(options["-ksp_max_it"].c_str());
+  if (options.count("-gpu_ilu_chunk")) opts_.ilu_chunk = std::atoi(options["-gpu_ilu_chunk"].c_str());
   if (options.count("-ksp_atol")) opts_.atol = std::atof(options["-ksp_atol"].c_str());
   if (options.count("-ksp_divtol")) opts_.dtol = std::atof(options["-ksp_divtol"].c_str());
   if (get("-gpu_precision", "fp64") == "mixed") opts_.precision = CFDGPU_PREC_MIXED;

@@ -3,27 +3,34 @@
 Mirrors the public methods of the reference's driver class
 (src/base/StabFEM.h:89-153) so a caller of the reference switches by changing
 the import.  Input formats are the reference's (see io.py); the solver-options
-file carries PETSc option names:
+file carries PETSc option names, with PETSc's defaults for a serial run:
 
-  -ksp_type gmres|preonly     -ksp_gmres_restart m    -ksp_rtol r
-  -ksp_atol a                 -ksp_divtol d           -ksp_max_it k
-  -pc_type jacobi|pbjacobi|none|bjacobi|lu
+  -ksp_type gmres|bcgs|preonly          -ksp_gmres_restart m (30)
+  -ksp_rtol r (1e-5)  -ksp_atol a (1e-50)  -ksp_divtol d (1e4)  -ksp_max_it k (10000)
+  -pc_type none|jacobi|pbjacobi|ilu|lu|bjacobi   (default ilu, PETSc's serial default)
+  -pc_factor_levels k                   (-pc_type ilu, default 0)
+  -sub_pc_type ilu|lu                   (-pc_type bjacobi, default ilu)
+  -sub_pc_factor_levels k               (-pc_type bjacobi with ILU blocks, default 0)
+  -pc_bjacobi_blocks B                  (default 1: one block per process, one process)
 
-plus this library's own keys:
+``-pc_type lu`` and ``-sub_pc_type lu`` are the library's complete block LU in
+natural ordering (the ILU machinery without a level limit), so the reference's
+tests (``-ksp_type preonly -pc_type lu``) run as direct solves; the
+``-pc_factor_mat_solver_type`` package name (MUMPS in the reference) is
+recorded but has no other effect.  An option value the library does not
+implement raises ``io.InputError`` instead of being replaced by another method.
+
+Library keys:
 
   -gpu_precision fp64|mixed   -gpu_inner_restart m    -gpu_inner_rtol r
   -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_newton_rtol r
+  -gpu_ilu_chunk R            (rows per warp task of the ILU triangular solves;
+                               scheduling only)
   -gpu_formulation semi_implicit|fully_implicit   (element routine; the
         reference's active one, or its commented-out fully-implicit one)
   -gpu_guess constant|extrapolation   (Newton initial guess; constant = the
                                        reference's, extrapolation = u_n plus
                                        the min-residual multiple of u_n - u_{n-1})
-
-The GPU library has no direct solver.  ``-ksp_type preonly -pc_type lu`` (the
-reference's shipped tests) is served by GMRES with point-block Jacobi at a
-tight tolerance, and ``-pc_type bjacobi`` (PETSc block Jacobi with ILU
-sub-solves) by point-block Jacobi; both substitutions are reported by
-``solver_description()``.
 """
 from __future__ import annotations
 
@@ -37,35 +44,41 @@ import numpy as np
 from . import io
 from ._lib import CfdGpuError, Handle
 
-# tolerance used when a direct solve is requested
-LU_SUBSTITUTE = {"restart": 300, "rtol": 1e-14, "atol": 1e-50, "max_it": 50000, "pc": "pbjacobi"}
-
 
 def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
-    """PETSc option dictionary -> keyword arguments of Handle (with PETSc defaults)."""
+    """PETSc option dictionary -> keyword arguments of Handle (with PETSc's
+    defaults for a serial run).  Raises io.InputError for a method the library
+    does not implement."""
     ksp = opts.get("-ksp_type", "gmres").lower()
-    pc = opts.get("-pc_type", "").lower()
-    kw = {"restart": 30, "rtol": 1e-5, "atol": 1e-50, "dtol": 1e4, "max_it": 10000, "pc": "pbjacobi"}
+    pc = opts.get("-pc_type", "ilu").lower()
+    kw = {"restart": 30, "rtol": 1e-5, "atol": 1e-50, "dtol": 1e4, "max_it": 10000, "ksp": "gmres"}
     notes: List[str] = []
-    if ksp == "preonly" or pc in ("lu", "cholesky"):
-        kw.update(LU_SUBSTITUTE)
-        notes.append("direct solve requested: GMRES(300)+pbjacobi at rtol 1e-14 substitutes")
+    if ksp not in ("gmres", "bcgs", "preonly"):
+        raise io.InputError(f"-ksp_type {ksp} is not implemented (gmres, bcgs, preonly)")
+    kw["ksp"] = ksp
+    if pc in ("none", "jacobi", "pbjacobi"):
+        kw["pc"] = pc
+    elif pc in ("ilu", "lu"):
+        kw.update(pc="bjacobi", bjacobi_blocks=1,
+                  ilu_levels=-1 if pc == "lu" else int(opts.get("-pc_factor_levels", "0")))
+    elif pc == "bjacobi":
+        sub = opts.get("-sub_pc_type", "ilu").lower()
+        if sub not in ("ilu", "lu"):
+            raise io.InputError(f"-sub_pc_type {sub} is not implemented (ilu, lu)")
+        sub_ksp = opts.get("-sub_ksp_type", "preonly").lower()
+        if sub_ksp != "preonly":
+            raise io.InputError(f"-sub_ksp_type {sub_ksp} is not implemented (preonly)")
+        kw.update(pc="bjacobi", bjacobi_blocks=int(opts.get("-pc_bjacobi_blocks", "1")),
+                  ilu_levels=-1 if sub == "lu" else int(opts.get("-sub_pc_factor_levels", "0")))
     else:
-        if ksp not in ("gmres", "fgmres"):
-            notes.append(f"-ksp_type {ksp} not available: GMRES used")
-        if pc in ("jacobi", "pbjacobi", "none"):
-            kw["pc"] = pc
-        elif pc in ("bjacobi", "asm", "ilu", ""):
-            kw["pc"] = "pbjacobi"
-            if pc:
-                notes.append(f"-pc_type {pc}: point-block Jacobi substitutes")
-        else:
-            notes.append(f"-pc_type {pc} not available: point-block Jacobi used")
-    if "-ksp_gmres_restart" in opts and ksp != "preonly":
+        raise io.InputError(f"-pc_type {pc} is not implemented (none, jacobi, pbjacobi, ilu, lu, bjacobi)")
+    if "-pc_factor_mat_solver_type" in opts:
+        notes.append(f"factorisation package {opts['-pc_factor_mat_solver_type']}: the library's block LU/ILU")
+    if "-ksp_gmres_restart" in opts:
         kw["restart"] = int(opts["-ksp_gmres_restart"])
     for key, name, conv in (("-ksp_rtol", "rtol", float), ("-ksp_atol", "atol", float),
                             ("-ksp_divtol", "dtol", float), ("-ksp_max_it", "max_it", int)):
-        if key in opts and not (ksp == "preonly" and name in ("rtol", "max_it")):
+        if key in opts:
             kw[name] = conv(opts[key])
     kw["precision"] = opts.get("-gpu_precision", "fp64")
     if "-gpu_inner_restart" in opts:
@@ -78,6 +91,8 @@ def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
         kw["refine_rtol"] = float(opts["-gpu_refine_rtol"])
     if "-gpu_newton_rtol" in opts:
         kw["newton_rtol"] = float(opts["-gpu_newton_rtol"])
+    if "-gpu_ilu_chunk" in opts:
+        kw["ilu_chunk"] = int(opts["-gpu_ilu_chunk"])
     if "-gpu_guess" in opts:
         kw["guess"] = opts["-gpu_guess"].lower()
     if "-gpu_formulation" in opts:
@@ -148,7 +163,13 @@ class StabFEM:
 
     def solver_description(self) -> str:
         k = self.solver_kw
-        s = f"GMRES({k['restart']}) pc={k['pc']} rtol={k['rtol']:g} max_it={k['max_it']} precision={k['precision']}"
+        ksp = {"gmres": f"GMRES({k['restart']})", "bcgs": "BCGS", "preonly": "preonly"}[k["ksp"]]
+        pc = k["pc"]
+        if pc == "bjacobi":
+            lev = k["ilu_levels"]
+            sub = "LU" if lev < 0 else f"ILU({lev})"
+            pc = f"bjacobi[{k['bjacobi_blocks']} x {sub}]"
+        s = f"{ksp} pc={pc} rtol={k['rtol']:g} max_it={k['max_it']} precision={k['precision']}"
         if k.get("guess", "constant") != "constant":
             s += f" guess={k['guess']}"
         if k.get("formulation", "semi_implicit") != "semi_implicit":

@@ -49,6 +49,17 @@ extern "C" {
 #define CFDGPU_PC_NONE 0
 #define CFDGPU_PC_JACOBI 1      /* inverse of the scalar diagonal */
 #define CFDGPU_PC_PBJACOBI 2    /* inverse of each node's ndof x ndof diagonal block */
+#define CFDGPU_PC_BJACOBI_ILU 3 /* -pc_type bjacobi -sub_pc_type ilu -sub_pc_factor_levels k
+                                   (input/petsc_options_gmres.dat:2-5): block Jacobi over
+                                   bjacobi_blocks contiguous node ranges, block ILU(ilu_levels)
+                                   in natural order inside each range; one range = -pc_type ilu */
+
+/* Krylov methods (PETSc -ksp_type names) */
+#define CFDGPU_KSP_GMRES 0      /* KSPGMRES: classical Gram-Schmidt, left preconditioning */
+#define CFDGPU_KSP_BCGS 1       /* KSPBCGS (input/petsc_options_bcgs.dat:1): BiCGStab, left preconditioning */
+#define CFDGPU_KSP_PREONLY 2    /* KSPPREONLY: x = M^-1 b, one preconditioner application; with the complete
+                                   factorisation (ilu_levels = -1, one block) a direct solve, as the
+                                   reference's tests ask (testdata/ldc2dquad10/petsc_options.dat:1-2) */
 
 /* precision modes */
 #define CFDGPU_PREC_FP64 0      /* FP64 element kernels, matrix and Krylov solve */
@@ -99,6 +110,12 @@ typedef struct cfdgpu_solver_opts {
   double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0||, F_0 the iteration-0
                                residual of the constant predictor (0: off, the reference's test only) */
   int formulation;          /* CFDGPU_FORM_*: element routine (0: the reference's active semi-implicit one) */
+  int ksp_type;             /* CFDGPU_KSP_* (0: GMRES) */
+  int ilu_levels;           /* CFDGPU_PC_BJACOBI_ILU: level of fill k (-sub_pc_factor_levels, 0..16); -1 keeps
+                               all fill: the complete block LU of each block (-pc_type lu, natural ordering) */
+  int bjacobi_blocks;       /* CFDGPU_PC_BJACOBI_ILU: number of blocks (0 or 1: one block, as a serial run) */
+  int ilu_chunk;            /* CFDGPU_PC_BJACOBI_ILU: rows per warp task in the triangular solves (0: 8; 1..32);
+                               scheduling only, results do not depend on it */
 } cfdgpu_solver_opts;
 
 /* element formulations */
@@ -202,6 +219,22 @@ int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double 
  * dofs).  its/reason may be NULL. */
 int cfdgpu_solve_export(cfdgpu_handle *h, const double *b, double *x, int *its, int *reason);
 
+/* Block ILU(k) factors of the last assembled matrix (handles with
+ * pc_type CFDGPU_PC_BJACOBI_ILU), for parity checks against a CPU ILU.  The
+ * factor pattern is a BSR over the nodes: rowptr (nNode+1), colidx (*nnzb,
+ * sorted per row), diag (nNode, position of each diagonal block); vals
+ * (nnzb*ndof*ndof, row-major blocks) hold the multipliers L_ip below the
+ * diagonal and U on and above it; dinv (nNode*ndof*ndof) the inverted
+ * diagonal blocks of U.  Any pointer may be NULL; asking for vals or dinv
+ * factorises the matrix first.  Replaces the numeric factorisation PETSc's
+ * PCSetUp runs inside KSPSolve (SolverPetsc.cpp:253). */
+int cfdgpu_ilu_export(cfdgpu_handle *h, int64_t *nnzb, int32_t *rowptr, int32_t *colidx, int32_t *diag, double *vals,
+                      double *dinv);
+
+/* z = M^-1 r with the handle's preconditioner, built from the last assembled
+ * matrix (PCApply; host arrays of nNode*ndof, zero at Dirichlet dofs). */
+int cfdgpu_pc_apply_export(cfdgpu_handle *h, const double *r, double *z);
+
 /* True (unpreconditioned) residual of the last assembled system:
  * *norm = ||b - A x||_2 with the library's deterministic reduction.  x and b
  * are host arrays of nNode*ndof doubles (zero at Dirichlet dofs). */
@@ -287,7 +320,10 @@ int cfdgpu_set_guess(cfdgpu_handle *h, cfdgpu_mpnn *m);
 #define CFDGPU_KIND_ELEM_K 1      /* element kernel, tangent + residual, one launch per colour */
 #define CFDGPU_KIND_ELEM_F 2      /* element kernel, residual only */
 #define CFDGPU_KIND_ORTHO 3       /* Gram-Schmidt multi-dot + update/norm pair */
-#define CFDGPU_KIND_COUNT 4
+#define CFDGPU_KIND_TRSV 4        /* block ILU triangular solves (lower + upper, one preconditioner application) */
+#define CFDGPU_KIND_ILU 5         /* block ILU numeric factorisation */
+#define CFDGPU_KIND_BCGS 6        /* BiCGStab vector updates and dot products of one iteration */
+#define CFDGPU_KIND_COUNT 7
 int cfdgpu_set_profiling(cfdgpu_handle *h, int on);
 /* Totals since profiling was switched on: launches, summed device ms, and
  * summed algorithmic bytes (the minimum DRAM traffic of each launch). */
