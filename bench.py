@@ -1,11 +1,12 @@
 """Benchmark: time steps/s of the 3D lid-driven-cavity hex8 solve on B200.
 
 One "step" is one time step of the solver (time update, boundary conditions,
-Newton loop with assembly and GMRES solves to the absolute 1e-8 residual).
-The default workload is the graded 32^3 hex8 cavity (32,768 elements, 35,937
-nodes, Re = 1000, dt = 0.1, generalised-alpha rho_inf = 0) with GMRES(400) and
-point-block Jacobi at rtol 1e-10.  W warm-up steps from rest run first, then
-exactly K timed steps.
+Newton loop with assembly and Krylov solves to the absolute 1e-8 residual).
+The default workload is the graded 115^3 hex8 cavity (1,520,875 elements,
+1,560,896 nodes, 6.24 M dofs, Re = 1000, dt = 0.1, generalised-alpha
+rho_inf = 0) with the reference's iterative option family: BiCGStab with a
+block-Jacobi ILU preconditioner (one block, as a single process) at rtol
+1e-10.  W warm-up steps from rest run first, then exactly K timed steps.
 
 Arms:
   default          the CUDA library through its C ABI (device-resident state);
@@ -33,13 +34,27 @@ sys.path.insert(0, ROOT)
 
 METRIC = "3D LDC hex8 time steps/s on 1 B200 (surrogate-guess vs plain) at 1e-8 residual"
 
-WORKLOADS = {
-    # name: (n per side, steps in the configuration, solver options)
-    "ldc3d_32": (32, 50, {"restart": 400, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 10000}),
-    "ldc3d_16": (16, 50, {"restart": 400, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 10000}),
-    "ldc3d_64": (64, 20, {"restart": 800, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 20000}),
-    "ldc3d_115": (115, 20, {"restart": 1000, "rtol": 1e-10, "pc": "pbjacobi", "max_it": 40000}),
+# Solver presets (Handle keywords).  The default is the reference's BiCGStab
+# option file (input/petsc_options_bcgs.dat) with one ILU(0) block;
+# "gmres-pbjacobi" is the point-block Jacobi GMRES used before the ILU
+# preconditioner existed (restart per workload).
+SOLVERS = {
+    "bcgs-ilu0": {"ksp": "bcgs", "pc": "bjacobi", "ilu_levels": 0, "rtol": 1e-10, "max_it": 10000},
+    "bcgs-ilu1": {"ksp": "bcgs", "pc": "bjacobi", "ilu_levels": 1, "rtol": 1e-10, "max_it": 10000},
+    "gmres20-ilu1": {"ksp": "gmres", "restart": 20, "pc": "bjacobi", "ilu_levels": 1, "rtol": 1e-10,
+                     "max_it": 10000},
+    "gmres-pbjacobi": {"ksp": "gmres", "pc": "pbjacobi", "rtol": 1e-10, "max_it": 40000},
 }
+DEFAULT_SOLVER = "bcgs-ilu0"
+
+WORKLOADS = {
+    # name: (n per side, steps in the configuration, GMRES restart of the pbjacobi preset)
+    "ldc3d_16": (16, 50, 400),
+    "ldc3d_32": (32, 50, 400),
+    "ldc3d_64": (64, 20, 800),
+    "ldc3d_115": (115, 20, 1000),
+}
+DEFAULT_WORKLOAD = "ldc3d_115"
 
 SMI_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -49,10 +64,11 @@ SMI_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.acti
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=4)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="ldc3d_32", choices=list(WORKLOADS))
+    p.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
+    p.add_argument("--solver", default=DEFAULT_SOLVER, choices=list(SOLVERS))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
@@ -81,14 +97,45 @@ def parse():
     return p.parse_args()
 
 
-def make_case(name, precision="fp64"):
+def solver_options(name, solver=DEFAULT_SOLVER):
+    opts = dict(SOLVERS[solver])
+    if solver == "gmres-pbjacobi":
+        opts["restart"] = WORKLOADS[name][2]
+    return opts
+
+
+def make_case(name, precision="fp64", solver=DEFAULT_SOLVER):
     from cfdsfemmpi_b200 import meshgen
-    n, steps, opts = WORKLOADS[name]
+    n, steps, _ = WORKLOADS[name]
     mesh, ctrl, _ = meshgen.case_hex(n, steps, mu=0.001, dt=0.1)
-    opts = dict(opts)
+    opts = solver_options(name, solver)
     if precision == "mixed":
-        opts.update(precision="mixed", inner_restart=100, inner_rtol=1e-4, max_it=40000)
+        opts = {"restart": WORKLOADS[name][2], "rtol": 1e-10, "pc": "pbjacobi", "precision": "mixed",
+                "inner_restart": 100, "inner_rtol": 1e-4, "max_it": 40000}
     return mesh, ctrl, opts
+
+
+def oracle_options(opts):
+    """OracleFEM keywords for the same solver as the Handle keywords `opts`."""
+    o = {"solver": opts.get("ksp", "gmres"), "rtol": opts["rtol"], "pc": opts["pc"],
+         "max_it": opts.get("max_it", 10000)}
+    if "restart" in opts:
+        o["restart"] = opts["restart"]
+    if opts["pc"] == "bjacobi":
+        o["ilu_levels"] = opts.get("ilu_levels", 0)
+        o["bjacobi_blocks"] = opts.get("bjacobi_blocks", 1)
+    return o
+
+
+def solver_label(opts):
+    ksp = opts.get("ksp", "gmres")
+    k = {"gmres": f"GMRES({opts.get('restart', 30)})", "bcgs": "BiCGStab", "preonly": "preonly"}[ksp]
+    if opts["pc"] == "bjacobi":
+        lev = opts.get("ilu_levels", 0)
+        pc = f"block Jacobi, {opts.get('bjacobi_blocks', 1)} block(s) of " + ("LU" if lev < 0 else f"ILU({lev})")
+    else:
+        pc = opts["pc"]
+    return f"{k} + {pc}, rtol {opts['rtol']:g}"
 
 
 def workload_config(name, mesh, opts, extra=None):
@@ -98,7 +145,7 @@ def workload_config(name, mesh, opts, extra=None):
            "method": ("plain (reference-identical constant predictor), FP64" if opts.get("precision", "fp64") == "fp64"
                       else "plain predictor, mixed precision: FP32 tangent + FP32 GMRES(100) cycles, FP64 refinement "
                            "and FP64 Newton residual"),
-           "solver": f"Newton to 1e-8 abs; GMRES({opts['restart']}) + {opts['pc']}, rtol {opts['rtol']:g}",
+           "solver": f"Newton to 1e-8 abs; {solver_label(opts)}",
            "l2": "flushed between timed steps (256 MiB write)"}
     if extra:
         cfg.update(extra)
@@ -174,13 +221,26 @@ def barrier_max(world, value):
     return float(t.item())
 
 
+KINDS = ("spmv", "ortho", "elem_k", "elem_f", "trsv", "ilu", "bcgs")
+
+# Work per timed step of the default workloads, as the GPU arm measures it on
+# steps W+1..W+K with W = 3 (the same algorithm as the CPU restatement): Newton
+# assemblies, linear solves, and Krylov iterations.  The reference arm scales
+# its bounded per-step sample with these counts; the GPU arm's own
+# cpu_baseline uses the live counts of its first timed step instead.
+STEP_WORK = {
+    ("ldc3d_115", "bcgs-ilu0"): (2, 1, 160),
+    ("ldc3d_115", "bcgs-ilu1"): (2, 1, 80),
+}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
     from cfdsfemmpi_b200 import Handle
 
     torch.cuda.set_device(local)
-    mesh, ctrl, opts = make_case(args.workload, args.precision)
+    mesh, ctrl, opts = make_case(args.workload, args.precision, args.solver)
     h = Handle(mesh, ctrl, **opts)
     stream = torch.cuda.ExternalStream(h.stream_ptr())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -199,6 +259,11 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         one_step(False)
     torch.cuda.synchronize()
+    # state at the start of the timed window: the end-to-end replay and the
+    # CPU sample start from it
+    s0 = h.get_solution()
+    p0, d0 = h.get_history()
+    t_start = timeNow
     launches0 = h.launch_count()
     sampler = ClockSampler(local)
     sampler.start()
@@ -223,22 +288,43 @@ def run_ours(args, world, rank, local):
     launches = h.launch_count() - launches0
     t_max = barrier_max(world, total_ms)
     value = world * args.steps / (t_max * 1e-3)
+    s_final = h.get_solution()
+
+    # end to end through the C ABI with host buffers: the same K time steps
+    # replayed on the same handle from the saved state; every step copies the
+    # state in from pinned host memory, steps, and copies the result back
+    # (cfdgpu_set_solution + cfdgpu_step + cfdgpu_get_solution)
+    e2e = None
+    if not args.no_e2e:
+        n = h.n
+        pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        pin.numpy()[:] = s0
+        h.set_history(p0, d0)
+        t2 = t_start
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            h.set_solution_ptr(pin.data_ptr())
+            h.step(t2, t2 if t2 <= 1.0 else 1.0)
+            t2 = t2 + ctrl.dt
+            h.get_solution_ptr(pin.data_ptr())
+        dt_e2e = time.perf_counter() - t0
+        dt_e2e = barrier_max(world, dt_e2e)
+        e2e = {"value": world * args.steps / dt_e2e, "unit": "steps/s", "steps": args.steps,
+               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+               "replay_bitwise_equal": bool(np.array_equal(pin.numpy(), s_final)),
+               "api": "cfdgpu_set_solution + cfdgpu_step + cfdgpu_get_solution (pinned host buffers), the same "
+                      "time steps as the device-resident timing replayed from the same state, host wall clock"}
 
     # dominant kernel: profile one more step with per-launch CUDA events
     h.set_profiling(True)
     one_step(False)
-    kinds = {k: h.kernel_stats(k) for k in ("spmv", "ortho", "elem_k", "elem_f")}
+    kinds = {k: h.kernel_stats(k) for k in KINDS}
     h.set_profiling(False)
     prof_total = sum(v[1] for v in kinds.values())
     dom = max(kinds, key=lambda k: kinds[k][1])
     nl, ms, by = kinds[dom]
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    peak, peak_src = _hbm_peak()
     achieved = (by / nl) / (ms / nl * 1e-3) / 1e9 if nl else None
     # DRAM traffic per launch: the ratio of ncu-measured DRAM bytes to
     # algorithmic bytes for this kernel kind and workload (profiles/), times
@@ -247,7 +333,7 @@ def run_ours(args, world, rank, local):
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath) and nl:
         try:
-            ent = json.load(open(tpath)).get(args.workload, {}).get(dom)
+            ent = json.load(open(tpath)).get(f"{args.workload}/{args.solver}", {}).get(dom)
             if ent:
                 traffic = ent["dram_bytes_per_algorithmic_byte"] * by / nl
         except Exception:
@@ -260,38 +346,11 @@ def run_ours(args, world, rank, local):
                 "kernels": {k: {"launches": v[0], "ms": round(v[1], 4),
                                 "gbs": (v[2] / (v[1] * 1e-3) / 1e9) if v[1] else None} for k, v in kinds.items()}}
 
-    # end to end through the C ABI with host buffers: a second handle replays
-    # the same steps (W warm-up, then the same K timed steps); every timed step
-    # copies the state in from pinned host memory, steps, and copies the
-    # result back (cfdgpu_set_solution + cfdgpu_step + cfdgpu_get_solution)
-    e2e = None
-    if not args.no_e2e:
-        h2 = Handle(mesh, ctrl, **opts)
-        n = h2.n
-        pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        t2 = ctrl.dt
-        for _ in range(args.warmup):
-            h2.step(t2, t2 if t2 <= 1.0 else 1.0)
-            t2 = t2 + ctrl.dt
-        h2.get_solution_ptr(pin.data_ptr())
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            h2.set_solution_ptr(pin.data_ptr())
-            h2.step(t2, t2 if t2 <= 1.0 else 1.0)
-            t2 = t2 + ctrl.dt
-            h2.get_solution_ptr(pin.data_ptr())
-        dt_e2e = time.perf_counter() - t0
-        h2.close()
-        dt_e2e = barrier_max(world, dt_e2e)
-        e2e = {"value": world * args.steps / dt_e2e, "unit": "steps/s", "steps": args.steps,
-               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
-               "api": "cfdgpu_set_solution + cfdgpu_step + cfdgpu_get_solution (pinned host buffers), "
-                      "same time steps as the device-resident timing, host wall clock"}
-
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(h, mesh, ctrl, opts, timeNow)
+        st0 = stats[0]
+        work = (st0["newton_iters"], len(st0["ksp_its"]), sum(st0["ksp_its"]))
+        cpu = cpu_baseline_sample(args, mesh, ctrl, opts, s0, d0, t_start, work)
     h.close()
     its = [sum(s["ksp_its"]) for s in stats]
     newt = [s["newton_iters"] for s in stats]
@@ -303,44 +362,108 @@ def run_ours(args, world, rank, local):
                                       {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                                        "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps} of the run"}),
             "newton_iters_per_step": statistics.mean(newt) if newt else None,
-            "gmres_iters_per_step": statistics.mean(its) if its else None,
-            "gmres_iters": its,
+            "krylov_iters_per_step": statistics.mean(its) if its else None,
+            "krylov_iters": its,
             "all_converged": all(s["converged"] for s in stats),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks}
     return line
 
 
-def cpu_baseline_sample(h, mesh, ctrl, opts, timeNow):
-    """Time one time step of the same run on the host cores with the CPU
-    restatement, starting from the GPU run's current state."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+def _cpu_sample_once(fem, ctrl, state, t_start, nits):
+    """Bounded sample of one time step on the host: the step's iteration-0
+    assembly, the preconditioner set-up (ILU factorisation) and `nits` Krylov
+    iterations of its linear solve.  Returns (t_assembly, t_setup, t_per_it)."""
     import numpy as np
     import oracle
-    threads = os.cpu_count() or 1
-    fem = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=opts["restart"], rtol=opts["rtol"],
-                           pc=opts["pc"], max_it=opts["max_it"], threads=threads)
-    fem.soln = h.get_solution()
-    _, fem.solnDot = h.get_history()
-    fem.timeNow = timeNow
+    s0, d0 = state
+    fem.soln = s0.copy()
+    fem.solnDot = d0.copy()
+    fem.timeNow = t_start
+    fem.td = oracle.time_params(ctrl.tis, ctrl.rhoInf, ctrl.dt)
+    fem.time_update()
+    tf = t_start if t_start <= 1.0 else 1.0
+    fem.solnApplied[fem.dbc_index] = fem.dbc_value * tf - fem.soln[fem.dbc_index]
+    fem.update_iter_step()
     t0 = time.perf_counter()
-    st = fem.step()
-    dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"one full time step (t = {timeNow:.1f}) of the same run from the GPU state; "
-                      f"{sum(st['gmres_its'])} GMRES its, {dt:.1f} s"}
+    fem.assemble(0)
+    t_asm = time.perf_counter() - t0
+    t_fac = 0.0
+    if fem.pc == 3:
+        t0 = time.perf_counter()
+        fem.factor_ilu()
+        t_fac = time.perf_counter() - t0
+    fem.max_it = nits
+    t0 = time.perf_counter()
+    _, info = fem.linear_solve()
+    t_lin = time.perf_counter() - t0
+    its = max(1, info["its"])
+    return t_asm, t_fac, max(0.0, t_lin - t_fac) / its, its
+
+
+def cpu_baseline_sample(args, mesh, ctrl, opts, s0, d0, t_start, work, nits=None):
+    """CPU restatement of the reference path (oracle/, OpenMP on all host
+    threads, the same solver) on a bounded sample of the first timed step,
+    scaled to a full step with that step's Newton/Krylov counts (the reference
+    reassembles the tangent every Newton iteration and sets the
+    preconditioner up for every solve)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    fem = oracle.OracleFEM(mesh, ctrl, **oracle_options(opts), threads=threads)
+    nits = nits or (10 if fem.solver == "bcgs" else opts.get("restart", 20))
+    t_asm, t_fac, t_it, its_done = _cpu_sample_once(fem, ctrl, (s0, d0), t_start, nits)
+    n_asm, n_solve, n_its = work
+    t_step = n_asm * t_asm + n_solve * t_fac + n_its * t_it
+    return {"value": 1.0 / t_step, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"time step t = {t_start:.1f} of the same run from the GPU state: iteration-0 assembly "
+                      f"{t_asm:.2f} s, preconditioner set-up {t_fac:.2f} s, {its_done} Krylov iterations at "
+                      f"{t_it:.3f} s each; scaled to the step's {n_asm} assemblies, {n_solve} set-ups and "
+                      f"{n_its} Krylov iterations = {t_step:.1f} s",
+            "t_assembly_s": t_asm, "t_setup_s": t_fac, "t_krylov_it_s": t_it}
 
 
 def run_reference(args, world, rank):
-    """CPU restatement of the reference path, all host threads."""
+    """CPU restatement of the reference path, all host threads.  Workloads up
+    to 64^3 run whole time steps; at 115^3 every step is a bounded sample
+    (assembly, preconditioner set-up and a few Krylov iterations of the
+    configuration's time step from rest) scaled with the measured work per
+    step of the same solver (STEP_WORK)."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
     import oracle
-    mesh, ctrl, opts = make_case(args.workload)
+    mesh, ctrl, opts = make_case(args.workload, args.precision, args.solver)
     threads = os.cpu_count() or 1
-    fem = oracle.OracleFEM(mesh, ctrl, solver="gmres", restart=opts["restart"], rtol=opts["rtol"], pc=opts["pc"],
-                           max_it=opts["max_it"], threads=threads)
+    fem = oracle.OracleFEM(mesh, ctrl, **oracle_options(opts), threads=threads)
+    bounded = (args.workload, args.solver) in STEP_WORK
+    base = {"metric": METRIC, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic: graded-cube hex8 cavity generated in-process (no dataset)",
+            "config": workload_config(args.workload, mesh, opts, {"parallelism": "host cores"})}
+    if bounded:
+        n_asm, n_solve, n_its = STEP_WORK[(args.workload, args.solver)]
+        zero = np.zeros(mesh.nNode * mesh.ndof)
+        samples = []
+        for k in range(args.warmup + args.steps):
+            r = _cpu_sample_once(fem, ctrl, (zero, zero), ctrl.dt, 10 if fem.solver == "bcgs" else 20)
+            if k >= args.warmup:
+                samples.append(r)
+        t_asm = statistics.mean(r[0] for r in samples)
+        t_fac = statistics.mean(r[1] for r in samples)
+        t_it = statistics.mean(r[2] for r in samples)
+        t_step = n_asm * t_asm + n_solve * t_fac + n_its * t_it
+        value = 1.0 / t_step
+        sample = (f"bounded sample per step (the first time step's iteration-0 assembly, ILU set-up and "
+                  f"{samples[0][3]} Krylov iterations, {args.steps} timed repeats after {args.warmup}), scaled to "
+                  f"{n_asm} assemblies, {n_solve} set-ups and {n_its} Krylov iterations per step (the work the GPU "
+                  f"arm measures per timed step with the same solver): {t_step:.1f} s per step")
+        line = dict(base, value=value, ms_per_step=t_step * 1e3,
+                    cpu_baseline={"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                                  "sample": sample, "t_assembly_s": t_asm, "t_setup_s": t_fac, "t_krylov_it_s": t_it},
+                    e2e={"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        return line
 
     def one():
         fem.step()
@@ -354,16 +477,12 @@ def run_reference(args, world, rank):
     dt = time.perf_counter() - t0
     stats = fem.stats[args.warmup:]
     value = args.steps / dt
-    return {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
-            "data": "synthetic: graded-cube hex8 cavity generated in-process (no dataset)",
-            "config": workload_config(args.workload, mesh, opts, {"parallelism": "host cores"}),
-            "gmres_iters_per_step": statistics.mean(sum(s["gmres_its"]) for s in stats),
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
-                             "sample": f"time steps {args.warmup + 1}..{args.warmup + args.steps} of the run, "
-                                       "C restatement (OpenMP) of the reference path"},
-            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return dict(base, value=value, ms_per_step=dt * 1e3 / args.steps,
+                krylov_iters_per_step=statistics.mean(sum(s["gmres_its"]) for s in stats),
+                cpu_baseline={"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                              "sample": f"time steps {args.warmup + 1}..{args.warmup + args.steps} of the run, "
+                                        "C restatement (OpenMP) of the reference path"},
+                e2e={"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
 
 
 GUESS_VARIANTS = {
@@ -700,9 +819,10 @@ def run_kernels(args, local):
     from cfdsfemmpi_b200 import Handle, meshgen
 
     torch.cuda.set_device(local)
-    n_side, _, opts = WORKLOADS[args.workload]
+    n_side = WORKLOADS[args.workload][0]
     mesh, ctrl, _ = meshgen.case_hex(n_side, 2)
-    kw = dict(opts, restart=args.kernel_restart, rtol=1e-30, max_it=args.kernel_its)
+    kw = dict(solver_options(args.workload, args.solver), restart=args.kernel_restart, rtol=1e-30,
+              max_it=args.kernel_its)
     h = Handle(mesh, ctrl, **kw)
     rng = np.random.default_rng(0)
     n = mesh.nNode * mesh.ndof
@@ -714,7 +834,7 @@ def run_kernels(args, local):
     b[h.export_pattern()["fixed_dofs"]] = 0.0
     x, its, reason = h.solve_export(b)
     dt = time.perf_counter() - t0
-    line = {"method": "kernels", "workload": args.workload, "nodes": mesh.nNode, "pc": kw["pc"],
+    line = {"method": "kernels", "workload": args.workload, "nodes": mesh.nNode, "solver": solver_label(kw),
             "restart": args.kernel_restart, "its": its, "reason": reason, "seconds": dt,
             "launches": h.launch_count()}
     h.close()

@@ -112,12 +112,13 @@ struct cfdgpu_handle {
   double prof_bytes[CFDGPU_KIND_COUNT] = {};
   // block-Jacobi ILU(k) preconditioner (pc_type CFDGPU_PC_BJACOBI_ILU)
   IluPattern ilu;
-  int32_t *frow = nullptr, *fcol = nullptr, *fdiag = nullptr, *faslot = nullptr;
+  int32_t *frow = nullptr, *fcol = nullptr, *fdiag = nullptr, *faslot = nullptr, *fumap = nullptr;
+  int32_t *florder = nullptr, *fuorder = nullptr;
+  int64_t *fuoff = nullptr;
   double *fval = nullptr, *fdinv = nullptr;
   unsigned int *iflags = nullptr;
   TriCtl *tctl = nullptr, *h_tctl = nullptr;
   double *ptmp = nullptr;          // A x before the triangular solves
-  int ilu_chunk = 8;
   // BiCGStab (ksp_type CFDGPU_KSP_BCGS)
   BcgsState *bst = nullptr, *h_bst = nullptr;
   double *bR = nullptr, *bRP = nullptr, *bP = nullptr, *bV = nullptr, *bS = nullptr, *bT = nullptr;
@@ -439,7 +440,7 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
 }
 
 // Persistent grid of the sync-free ILU kernels: enough warps for `tasks`
-// tasks, at most 4 CTAs of 8 warps per SM.
+// rows, at most 4 CTAs of 8 warps per SM.
 static inline int ilu_grid(int64_t tasks)
 {
   const int64_t ctas = (tasks + ILU_WARPS - 1) / ILU_WARPS;
@@ -448,9 +449,10 @@ static inline int ilu_grid(int64_t tasks)
 
 static double ilu_factor_bytes(cfdgpu_handle *h)
 {
-  // read A once, write the factors and the inverted diagonals once
+  // read A and the update map once, write the factors and the inverted diagonals once
   const double bb = (double)h->ndof * h->ndof * 8.0;
-  return (double)h->topo.nnzb() * bb + (double)h->ilu.nnzb() * bb + (double)h->nNode * bb;
+  return (double)h->topo.nnzb() * bb + (double)h->ilu.nnzb() * bb + (double)h->nNode * bb +
+         4.0 * (double)h->ilu.umap.size();
 }
 
 static double trsv_bytes(cfdgpu_handle *h)
@@ -468,12 +470,12 @@ static int ilu_factor_run(cfdgpu_handle *h)
   const int grid = ilu_grid(h->nNode);
   if (h->ndof == 4)
     ilu_factor<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
-                                                                      h->fcol, h->fdiag, h->fval, h->fdinv, h->iflags,
-                                                                      h->tctl);
+                                                                      h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                      h->fval, h->fdinv, h->iflags, h->tctl);
   else
     ilu_factor<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
-                                                                      h->fcol, h->fdiag, h->fval, h->fdinv, h->iflags,
-                                                                      h->tctl);
+                                                                      h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                      h->fval, h->fdinv, h->iflags, h->tctl);
   prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "ilu_factor");
@@ -483,20 +485,19 @@ static int ilu_factor_run(cfdgpu_handle *h)
 static int ilu_apply(cfdgpu_handle *h, const double *r, double *z, const GmresState *st, int j, const int *active)
 {
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, trsv_bytes(h));
-  const int chunk = h->ilu_chunk;
-  const int grid = ilu_grid((h->nNode + chunk - 1) / chunk);
+  const int grid = ilu_grid(h->nNode);
   if (h->ndof == 4) {
-    ilu_lsolve<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
-                                                                      h->fval, r, z, h->iflags, h->tctl, st, j, active);
-    ilu_usolve<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
-                                                                      h->fval, h->fdinv, z, z, h->iflags, h->tctl, st,
-                                                                      j, active);
+    ilu_trsv<4, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, r, z, h->iflags, h->tctl, st, j, active);
+    ilu_trsv<4, true, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, nullptr, z, h->iflags, h->tctl, st, j,
+        active);
   } else {
-    ilu_lsolve<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
-                                                                      h->fval, r, z, h->iflags, h->tctl, st, j, active);
-    ilu_usolve<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, chunk, h->frow, h->fcol, h->fdiag,
-                                                                      h->fval, h->fdinv, z, z, h->iflags, h->tctl, st,
-                                                                      j, active);
+    ilu_trsv<3, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, r, z, h->iflags, h->tctl, st, j, active);
+    ilu_trsv<3, true, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, nullptr, z, h->iflags, h->tctl, st, j,
+        active);
   }
   prof_end(h, pi);
   h->launches += 2;
@@ -1103,11 +1104,6 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
       h->err = "the block ILU preconditioner runs in FP64 precision mode";
       return CFDGPU_EINVAL;
     }
-    if (h->opts.ilu_chunk < 0 || h->opts.ilu_chunk > ILU_MAX_CHUNK) {
-      h->err = "ilu_chunk must lie in [0, 32]";
-      return CFDGPU_EINVAL;
-    }
-    h->ilu_chunk = (h->opts.ilu_chunk > 0) ? h->opts.ilu_chunk : 8;
   }
   if (h->opts.ksp_type != CFDGPU_KSP_GMRES && h->opts.precision != CFDGPU_PREC_FP64) {
     h->err = "BiCGStab and preonly run in FP64 precision mode";
@@ -1229,6 +1225,10 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = upload(h, &h->fcol, f.colidx.data(), f.colidx.size()))) return rc;
     if ((rc = upload(h, &h->fdiag, f.diag.data(), f.diag.size()))) return rc;
     if ((rc = upload(h, &h->faslot, f.aslot.data(), f.aslot.size()))) return rc;
+    if ((rc = upload(h, &h->fuoff, f.uoff.data(), f.uoff.size()))) return rc;
+    if ((rc = upload(h, &h->fumap, f.umap.data(), f.umap.size()))) return rc;
+    if ((rc = upload(h, &h->florder, f.lorder.data(), f.lorder.size()))) return rc;
+    if ((rc = upload(h, &h->fuorder, f.uorder.data(), f.uorder.size()))) return rc;
     if ((rc = dalloc(h, &h->fval, (size_t)f.nnzb() * bb))) return rc;
     CK(cudaMemset(h->fval, 0, sizeof(double) * f.nnzb() * bb));
     if ((rc = dalloc(h, &h->fdinv, (size_t)h->nNode * bb))) return rc;

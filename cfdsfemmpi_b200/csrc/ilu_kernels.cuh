@@ -9,18 +9,20 @@
 // Strictly lower blocks hold the multipliers L_ip (unit block-lower factor),
 // the others U_ij; fdinv[i] holds the inverse of U_ii (pivoted Gauss-Jordan).
 //
-// Scheduling is sync-free: one persistent grid whose warps draw consecutive
-// row chunks from an atomic ticket (ascending rows for the factorisation and
-// the lower solve, descending for the upper solve).  A chunk whose rows need
-// rows of another chunk waits on that chunk's flag (acquire load), and a
-// finished chunk publishes its flag with a release store.  Tickets are drawn
-// in dependency order by running warps, so the earliest unfinished chunk
-// always has its inputs and progress is guaranteed; every wait is bounded and
-// records a time-out in the control block instead of spinning forever.  Flags
-// hold an epoch number: the last warp of a launch resets the ticket and
-// advances the epoch, so no per-launch reset kernel is needed and launches
-// can be captured in CUDA graphs.  Every row's arithmetic runs in a fixed
-// order, so results do not depend on scheduling.
+// Scheduling is sync-free: one persistent grid whose warps draw rows from an
+// atomic ticket in level-set order (the levels of the factorisation / lower
+// solve DAG for the factorisation and the lower solve, of the upper solve DAG
+// for the upper solve, computed on the host).  Rows of one level are
+// independent, so a row only waits for rows handed out before it: a row whose
+// inputs are not ready polls their flags (relaxed loads with back-off, then
+// one acquire fence), and a finished row publishes its flag with a release
+// store.  The earliest unfinished row always has its inputs, so progress is
+// guaranteed; every wait is bounded and records a time-out in the control
+// block instead of spinning forever.  Flags hold an epoch number: the last
+// warp of a launch resets the ticket and advances the epoch, so no per-launch
+// reset kernel is needed and launches can be captured in CUDA graphs.  Every
+// row's arithmetic runs in a fixed order, so results do not depend on
+// scheduling.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -41,7 +43,6 @@ constexpr unsigned int ILU_ERR_TIMEOUT = 1u;     // a dependency wait ran out (n
 constexpr unsigned int ILU_ERR_ZERO_PIVOT = 2u;  // singular diagonal block in the factorisation
 constexpr int ILU_THREADS = 256;
 constexpr int ILU_WARPS = ILU_THREADS / 32;
-constexpr int ILU_MAX_CHUNK = 32;
 constexpr int ILU_SPIN_LIMIT = 1 << 21;          // ~1-2 s of polling per wait
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p)
@@ -56,14 +57,27 @@ __device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v)
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Wait until *f == target (bounded).  Returns false after a time-out, or when
-// another warp has already timed out.
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int *p)
+{
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Wait until *f == target (bounded): relaxed polls with exponential back-off.
+// The caller completes the acquire with fence_acq_rel_gpu() after the polls
+// of all its lanes (one fence per row instead of one acquire per input).
+// Returns false after a time-out, or when another warp has already timed out.
 __device__ __forceinline__ bool wait_flag(const unsigned int *f, unsigned int target, TriCtl *ctl)
 {
-  if (ld_acquire_u32(f) == target) return true;
+  if (ld_relaxed_u32(f) == target) return true;
+  unsigned int ns = 32;
   for (int it = 0; it < ILU_SPIN_LIMIT; it++) {
-    __nanosleep(64);
-    if (ld_acquire_u32(f) == target) return true;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+    if (ld_relaxed_u32(f) == target) return true;
     if (*(volatile unsigned int *)&ctl->error) return false;
   }
   atomicCAS(&ctl->error, 0u, ILU_ERR_TIMEOUT);
@@ -99,18 +113,6 @@ template <typename T>
 __device__ __forceinline__ double ld_cg(const T *p)
 {
   return (double)__ldcg(p);
-}
-
-// position of column j in fcol[lo, hi) (sorted), or -1
-__device__ __forceinline__ int find_col(const int32_t *__restrict__ fcol, int lo, int hi, int j)
-{
-  const int end = hi;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (fcol[mid] < j) lo = mid + 1;
-    else hi = mid;
-  }
-  return (lo < end && fcol[lo] == j) ? lo : -1;
 }
 
 // Invert an NB x NB block (row-major, FP64) with partial pivoting; returns
@@ -156,13 +158,15 @@ __device__ __forceinline__ bool invert_block(double (&A)[NB][NB], double (&I)[NB
 // Numeric block ILU: one warp per node row, rows in ascending order.  For row
 // i: W = the row of A on the factor pattern (fill blocks zero); for every
 // pivot p < i of the row in increasing column order, L_ip = W_p U_pp^-1 and
-// W_j -= L_ip U_pj for the blocks j > p of row p that lie in row i's pattern;
-// then U_ii^-1.  AT is the type of the assembled matrix, FT of the factors
+// W_j -= L_ip U_pj for the blocks j > p of row p that lie in row i's pattern
+// (their positions come from the symbolic phase's update map); then
+// U_ii^-1.  AT is the type of the assembled matrix, FT of the factors
 // (FP64 arithmetic in both cases).
 template <int NB, typename AT, typename FT>
 __global__ void __launch_bounds__(ILU_THREADS)
 ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ aslot, const AT *__restrict__ aval,
            const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol, const int32_t *__restrict__ fdiag,
+           const int64_t *__restrict__ uoff, const int32_t *__restrict__ umap, const int32_t *__restrict__ order,
            FT *fval, FT *fdinv, unsigned int *flags, TriCtl *ctl)
 {
   constexpr int BB = NB * NB;
@@ -173,8 +177,9 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
   const unsigned int target = epoch + 1u;
   const int g = lane / BB, e = lane % BB, er = e / NB, ec = e % NB;
   while (true) {
-    const int i = draw_ticket(ctl, lane);
-    if (i >= n) break;
+    const int tk = draw_ticket(ctl, lane);
+    if (tk >= n) break;
+    const int i = order[tk];
     const int f0 = fptr[i], f1 = fptr[i + 1], fd = fdiag[i];
     for (int64_t x = (int64_t)f0 * BB + lane; x < (int64_t)f1 * BB; x += 32) fval[x] = FT(0);
     __syncwarp();
@@ -191,6 +196,7 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
       const int p = fcol[q];
       if (lane == 0) wait_flag(flags + p, target, ctl);
       __syncwarp();
+      fence_acq_rel_gpu();
       if (lane < BB) {
         double s = 0.0;
 #pragma unroll
@@ -201,16 +207,31 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
       __syncwarp();
       if (lane < BB) fval[(int64_t)q * BB + lane] = (FT)Lsh[w][lane];
       const int u0 = fdiag[p] + 1, u1 = fptr[p + 1];
-      for (int t0 = u0; t0 < u1; t0 += G) {
-        const int t = t0 + g;
-        if (g < G && t < u1) {
-          const int j = fcol[t];
-          const int pos = find_col(fcol, q + 1, f1, j);
-          if (pos >= 0) {
+      const int32_t *__restrict__ map = umap + uoff[q] - u0;
+      double lrow[NB];
+#pragma unroll
+      for (int k = 0; k < NB; k++) lrow[k] = Lsh[w][er * NB + k];
+      // UNR independent blocks per lane group in flight: all loads first,
+      // then the updates (each target block is written by one lane group)
+      constexpr int UNR = 4;
+      for (int t0 = u0; t0 < u1; t0 += G * UNR) {
+        int pos[UNR];
+        double ub[UNR][NB];
+#pragma unroll
+        for (int r = 0; r < UNR; r++) {
+          const int t = t0 + r * G + g;
+          pos[r] = (g < G && t < u1) ? map[t] : -1;
+#pragma unroll
+          for (int k = 0; k < NB; k++)
+            ub[r][k] = (pos[r] >= 0) ? ld_cg(fval + (int64_t)t * BB + k * NB + ec) : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < UNR; r++) {
+          if (pos[r] >= 0) {
             double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < NB; k++) s = fma(Lsh[w][er * NB + k], ld_cg(fval + (int64_t)t * BB + k * NB + ec), s);
-            fval[(int64_t)pos * BB + e] = (FT)((double)fval[(int64_t)pos * BB + e] - s);
+            for (int k = 0; k < NB; k++) s = fma(lrow[k], ub[r][k], s);
+            fval[(int64_t)pos[r] * BB + e] = (FT)((double)fval[(int64_t)pos[r] * BB + e] - s);
           }
         }
       }
@@ -230,147 +251,89 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
 #pragma unroll
         for (int c = 0; c < NB; c++) fdinv[(int64_t)i * BB + a * NB + c] = (FT)I[a][c];
     }
+    // every lane's writes of the row are visible before the flag
+    __threadfence();
     __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      st_release_u32(flags + i, target);
-    }
+    if (lane == 0) st_release_u32(flags + i, target);
   }
   launch_done(ctl, lane, epoch);
 }
 
 // ---------------------------------------------------------------------------
-// Triangular solves z = (L U)^-1 r.  A warp takes a chunk of `chunk`
-// consecutive rows (ascending for L, descending for U) and solves them in
-// order, keeping the chunk's results in shared memory; rows of other chunks
-// are read after their chunk's flag (one flag per chunk).
+// Triangular solves z = (L U)^-1 r, one warp per row, rows in level order
+// (lorder for the lower solve, uorder for the upper solve).  The lanes poll
+// the row's dependencies (one flag per row), accumulate the off-diagonal
+// products (32 / NB^2 blocks per warp step, fixed order), and lane 0 stores
+// the row's NB values and then its flag with a release store.
 //
 // Lower:  y_i = r_i - sum_{p<i} L_ip y_p              (in place over r allowed)
 // Upper:  z_i = U_ii^-1 (y_i - sum_{p>i} U_ip z_p)   (in place over y allowed)
 // st/j: inside a GMRES chunk the launch is skipped once the cycle has ended;
 // active: inside a BiCGStab chunk, once the solve has ended.
-template <int NB, typename FT, typename VT>
+template <int NB, bool UPPER, typename FT, typename VT>
 __global__ void __launch_bounds__(ILU_THREADS)
-ilu_lsolve(int n, int chunk, const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol,
-           const int32_t *__restrict__ fdiag, const FT *__restrict__ fval, const VT *r, VT *y, unsigned int *flags,
-           TriCtl *ctl, const GmresState *__restrict__ st, int j, const int *__restrict__ active)
+ilu_trsv(int n, const int32_t *__restrict__ order, const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol,
+         const int32_t *__restrict__ fdiag, const FT *__restrict__ fval, const FT *__restrict__ fdinv, const VT *r,
+         VT *y, unsigned int *flags, TriCtl *ctl, const GmresState *__restrict__ st, int j,
+         const int *__restrict__ active)
 {
   if (st && (!st->active || st->it != j)) return;
   if (active && !active[0]) return;
   constexpr int BB = NB * NB;
   constexpr int G = 32 / BB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  __shared__ double ych[ILU_WARPS][ILU_MAX_CHUNK * NB];
   __shared__ double red[ILU_WARPS][32];
   const unsigned int epoch = *(volatile unsigned int *)&ctl->epoch;
   const unsigned int target = epoch + 1u;
   const int g = lane / BB, e = lane % BB, ec = e % NB;
-  const int nchunks = (n + chunk - 1) / chunk;
   while (true) {
-    const int t = draw_ticket(ctl, lane);
-    if (t >= nchunks) break;
-    const int i0 = t * chunk, i1 = min(n, i0 + chunk);
-    for (int i = i0; i < i1; i++) {
-      const int q0 = fptr[i], q1 = fdiag[i];
-      for (int q = q0 + lane; q < q1; q += 32) {
+    const int tk = draw_ticket(ctl, lane);
+    if (tk >= n) break;
+    const int i = order[tk];
+    const int q0 = UPPER ? fdiag[i] + 1 : fptr[i];
+    const int q1 = UPPER ? fptr[i + 1] : fdiag[i];
+    for (int q = q0 + lane; q < q1; q += 32) wait_flag(flags + fcol[q], target, ctl);
+    __syncwarp();
+    fence_acq_rel_gpu();
+    double acc = 0.0;
+    for (int qb = q0; qb < q1; qb += G) {
+      const int q = qb + g;
+      if (g < G && q < q1) {
         const int p = fcol[q];
-        if (p < i0) wait_flag(flags + p / chunk, target, ctl);
+        acc = fma((double)fval[(int64_t)q * BB + e], ld_cg(y + (int64_t)p * NB + ec), acc);
       }
-      __syncwarp();
-      double acc = 0.0;
-      for (int qb = q0; qb < q1; qb += G) {
-        const int q = qb + g;
-        if (g < G && q < q1) {
-          const int p = fcol[q];
-          const double yp = (p >= i0) ? ych[w][(p - i0) * NB + ec] : ld_cg(y + (int64_t)p * NB + ec);
-          acc = fma((double)fval[(int64_t)q * BB + e], yp, acc);
-        }
-      }
-      red[w][lane] = acc;
-      __syncwarp();
-      if (lane < NB) {
-        double s = (double)r[(int64_t)i * NB + lane];
-#pragma unroll
-        for (int gg = 0; gg < G; gg++)
-#pragma unroll
-          for (int c = 0; c < NB; c++) s -= red[w][gg * BB + lane * NB + c];
-        ych[w][(i - i0) * NB + lane] = s;
-        y[(int64_t)i * NB + lane] = (VT)s;
-      }
-      __syncwarp();
     }
-    if (lane == 0) {
-      __threadfence();
-      st_release_u32(flags + t, target);
+    red[w][lane] = acc;
+    __syncwarp();
+    double s = 0.0;
+    if (lane < NB) {
+      s = UPPER ? ld_cg(y + (int64_t)i * NB + lane) : (double)r[(int64_t)i * NB + lane];
+#pragma unroll
+      for (int gg = 0; gg < G; gg++)
+#pragma unroll
+        for (int c = 0; c < NB; c++) s -= red[w][gg * BB + lane * NB + c];
     }
-  }
-  launch_done(ctl, lane, epoch);
-}
-
-template <int NB, typename FT, typename VT>
-__global__ void __launch_bounds__(ILU_THREADS)
-ilu_usolve(int n, int chunk, const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol,
-           const int32_t *__restrict__ fdiag, const FT *__restrict__ fval, const FT *__restrict__ fdinv, const VT *y,
-           VT *z, unsigned int *flags, TriCtl *ctl, const GmresState *__restrict__ st, int j,
-           const int *__restrict__ active)
-{
-  if (st && (!st->active || st->it != j)) return;
-  if (active && !active[0]) return;
-  constexpr int BB = NB * NB;
-  constexpr int G = 32 / BB;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  __shared__ double zch[ILU_WARPS][ILU_MAX_CHUNK * NB];
-  __shared__ double red[ILU_WARPS][32];
-  __shared__ double sv[ILU_WARPS][NB];
-  const unsigned int epoch = *(volatile unsigned int *)&ctl->epoch;
-  const unsigned int target = epoch + 1u;
-  const int g = lane / BB, e = lane % BB, ec = e % NB;
-  const int nchunks = (n + chunk - 1) / chunk;
-  while (true) {
-    const int t = draw_ticket(ctl, lane);
-    if (t >= nchunks) break;
-    // chunk t covers rows hi, hi-1, ..., lo
-    const int hi = n - 1 - t * chunk, lo = max(0, hi - chunk + 1);
-    for (int i = hi; i >= lo; i--) {
-      const int q0 = fdiag[i] + 1, q1 = fptr[i + 1];
-      for (int q = q0 + lane; q < q1; q += 32) {
-        const int p = fcol[q];
-        if (p > hi) wait_flag(flags + (n - 1 - p) / chunk, target, ctl);
-      }
-      __syncwarp();
-      double acc = 0.0;
-      for (int qb = q0; qb < q1; qb += G) {
-        const int q = qb + g;
-        if (g < G && q < q1) {
-          const int p = fcol[q];
-          const double zp = (p <= hi) ? zch[w][(hi - p) * NB + ec] : ld_cg(z + (int64_t)p * NB + ec);
-          acc = fma((double)fval[(int64_t)q * BB + e], zp, acc);
-        }
-      }
-      red[w][lane] = acc;
-      __syncwarp();
-      if (lane < NB) {
-        double s = ld_cg(y + (int64_t)i * NB + lane);
+    if (UPPER) {
+      // z_i = U_ii^-1 s: lane a takes row a of the inverse
+      double sv[NB];
 #pragma unroll
-        for (int gg = 0; gg < G; gg++)
-#pragma unroll
-          for (int c = 0; c < NB; c++) s -= red[w][gg * BB + lane * NB + c];
-        sv[w][lane] = s;
-      }
-      __syncwarp();
+      for (int c = 0; c < NB; c++) sv[c] = __shfl_sync(0xffffffffu, s, c);
       if (lane < NB) {
         double v = 0.0;
 #pragma unroll
-        for (int c = 0; c < NB; c++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + c], sv[w][c], v);
-        zch[w][(hi - i) * NB + lane] = v;
-        z[(int64_t)i * NB + lane] = (VT)v;
+        for (int c = 0; c < NB; c++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + c], sv[c], v);
+        s = v;
       }
-      __syncwarp();
     }
+    double out[NB];
+#pragma unroll
+    for (int c = 0; c < NB; c++) out[c] = __shfl_sync(0xffffffffu, s, c);
     if (lane == 0) {
-      __threadfence();
-      st_release_u32(flags + t, target);
+#pragma unroll
+      for (int c = 0; c < NB; c++) y[(int64_t)i * NB + c] = (VT)out[c];
+      st_release_u32(flags + i, target);
     }
+    __syncwarp();
   }
   launch_done(ctl, lane, epoch);
 }

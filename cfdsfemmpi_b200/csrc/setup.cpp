@@ -214,6 +214,54 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
     f.rowptr[i + 1] = (int32_t)f.colidx.size();
     if (f.diag[i] < 0) return "node without a diagonal block";
   }
+  // level-set orders of the lower and upper dependency DAGs
+  {
+    std::vector<int32_t> lev(n, 0);
+    auto order_by = [&](std::vector<int32_t> &out) {
+      int nl = 0;
+      for (int i = 0; i < n; i++) nl = std::max(nl, lev[i] + 1);
+      std::vector<int32_t> cnt(nl + 1, 0);
+      for (int i = 0; i < n; i++) cnt[lev[i] + 1]++;
+      for (int k = 0; k < nl; k++) cnt[k + 1] += cnt[k];
+      out.resize(n);
+      for (int i = 0; i < n; i++) out[cnt[lev[i]]++] = i;
+      return nl;
+    };
+    for (int i = 0; i < n; i++) {
+      int d = 0;
+      for (int q = f.rowptr[i]; q < f.diag[i]; q++) d = std::max(d, lev[f.colidx[q]] + 1);
+      lev[i] = d;
+    }
+    f.nlev_l = order_by(f.lorder);
+    for (int i = n - 1; i >= 0; i--) {
+      int d = 0;
+      for (int q = f.diag[i] + 1; q < f.rowptr[i + 1]; q++) d = std::max(d, lev[f.colidx[q]] + 1);
+      lev[i] = d;
+    }
+    f.nlev_u = order_by(f.uorder);
+  }
+  // update map: positions in row i of the upper blocks of every pivot row
+  {
+    int64_t total = 0;
+    f.uoff.assign(f.colidx.size(), -1);
+    for (int i = 0; i < n; i++)
+      for (int q = f.rowptr[i]; q < f.diag[i]; q++) {
+        const int p = f.colidx[q];
+        f.uoff[q] = total;
+        total += f.rowptr[p + 1] - f.diag[p] - 1;
+      }
+    f.umap.resize(total);
+    std::vector<int32_t> pos(n, -1);
+    for (int i = 0; i < n; i++) {
+      for (int k = f.rowptr[i]; k < f.rowptr[i + 1]; k++) pos[f.colidx[k]] = k;
+      for (int q = f.rowptr[i]; q < f.diag[i]; q++) {
+        const int p = f.colidx[q];
+        int64_t o = f.uoff[q];
+        for (int u = f.diag[p] + 1; u < f.rowptr[p + 1]; u++) f.umap[o++] = pos[f.colidx[u]];
+      }
+      for (int k = f.rowptr[i]; k < f.rowptr[i + 1]; k++) pos[f.colidx[k]] = -1;
+    }
+  }
   // blocks of A inside the factor pattern
   f.aslot.assign(t.colidx.size(), -1);
   for (int i = 0; i < n; i++) {

@@ -60,6 +60,16 @@ struct IluPattern {
   std::vector<int32_t> diag;     // position of the diagonal block of each row
   std::vector<int32_t> aslot;    // per block of A: its position in the factors, or -1
   std::vector<int32_t> blk;      // nblocks+1 node offsets
+  // update map of the numeric factorisation: for a strictly lower block q =
+  // (i, p), umap[uoff[q] + k] is the position in row i of the k-th block
+  // right of the diagonal in row p, or -1 when row i's pattern drops it
+  std::vector<int64_t> uoff;     // nnzb (meaningful for strictly lower blocks)
+  std::vector<int32_t> umap;
+  // rows sorted by level of the lower DAG (factorisation and lower solve:
+  // level(i) = 1 + max level of the strictly lower blocks' columns) and of
+  // the upper DAG (upper solve), row order inside a level
+  std::vector<int32_t> lorder, uorder;
+  int nlev_l = 0, nlev_u = 0;
   int64_t nnzb() const { return (int64_t)colidx.size(); }
 };
 

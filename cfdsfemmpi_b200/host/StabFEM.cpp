@@ -187,7 +187,6 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
   if (options.count("-ksp_gmres_restart")) opts_.restart = std::atoi(options["-ksp_gmres_restart"].c_str());
   if (options.count("-ksp_rtol")) opts_.rtol = std::atof(options["-ksp_rtol"].c_str());
   if (options.count("-ksp_max_it")) opts_.max_it = std::atoi(options["-ksp_max_it"].c_str());
-  if (options.count("-gpu_ilu_chunk")) opts_.ilu_chunk = std::atoi(options["-gpu_ilu_chunk"].c_str());
   if (options.count("-ksp_atol")) opts_.atol = std::atof(options["-ksp_atol"].c_str());
   if (options.count("-ksp_divtol")) opts_.dtol = std::atof(options["-ksp_divtol"].c_str());
   if (get("-gpu_precision", "fp64") == "mixed") opts_.precision = CFDGPU_PREC_MIXED;

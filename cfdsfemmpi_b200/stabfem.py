@@ -24,8 +24,6 @@ Library keys:
 
   -gpu_precision fp64|mixed   -gpu_inner_restart m    -gpu_inner_rtol r
   -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_newton_rtol r
-  -gpu_ilu_chunk R            (rows per warp task of the ILU triangular solves;
-                               scheduling only)
   -gpu_formulation semi_implicit|fully_implicit   (element routine; the
         reference's active one, or its commented-out fully-implicit one)
   -gpu_guess constant|extrapolation   (Newton initial guess; constant = the
@@ -91,8 +89,6 @@ def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
         kw["refine_rtol"] = float(opts["-gpu_refine_rtol"])
     if "-gpu_newton_rtol" in opts:
         kw["newton_rtol"] = float(opts["-gpu_newton_rtol"])
-    if "-gpu_ilu_chunk" in opts:
-        kw["ilu_chunk"] = int(opts["-gpu_ilu_chunk"])
     if "-gpu_guess" in opts:
         kw["guess"] = opts["-gpu_guess"].lower()
     if "-gpu_formulation" in opts:
@@ -123,6 +119,7 @@ class StabFEM:
         self._soln_cache: Optional[np.ndarray] = None
         self.write_vtu = False
         self.write_forces = True
+        self.last_error = ""
 
     def _print(self, *a):
         if self.verbose:
@@ -195,6 +192,7 @@ class StabFEM:
             try:
                 st = h.step(timeNow, timeFact).as_dict()
             except CfdGpuError as e:
+                self.last_error = str(e)
                 self._print(" PETSc solver not converged. \n\n" if e.code == -4 else str(e))
                 rc = -1
                 break

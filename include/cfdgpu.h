@@ -114,8 +114,6 @@ typedef struct cfdgpu_solver_opts {
   int ilu_levels;           /* CFDGPU_PC_BJACOBI_ILU: level of fill k (-sub_pc_factor_levels, 0..16); -1 keeps
                                all fill: the complete block LU of each block (-pc_type lu, natural ordering) */
   int bjacobi_blocks;       /* CFDGPU_PC_BJACOBI_ILU: number of blocks (0 or 1: one block, as a serial run) */
-  int ilu_chunk;            /* CFDGPU_PC_BJACOBI_ILU: rows per warp task in the triangular solves (0: 8; 1..32);
-                               scheduling only, results do not depend on it */
 } cfdgpu_solver_opts;
 
 /* element formulations */

@@ -1,0 +1,79 @@
+"""Field parity on the graded 32^3 lid-driven cavity with the benchmark's
+solver options (Re 1000, dt 0.1, gen-alpha rho_inf 0, Newton to 1e-8).
+
+The GPU run and the oracle solve every Newton system to the same relative
+(preconditioned) Krylov tolerance, so their fields can differ by about
+cond(A) * rtol even when both are correct: summation order alone moves the
+answer.  The test measures that floor instead of assuming it: the oracle runs
+twice with different summation orders (one host thread, which also assembles
+in the reference's element order, against all host threads, which assemble
+colour by colour and split every dot product), and the GPU must agree with
+the oracle to max(1e-8, 2 x that spread).  Set CFDGPU_PARITY_RECORD to a file
+path to append the measured numbers as one JSON line.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import bench
+import oracle
+from cfdsfemmpi_b200 import Handle
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(mesh, ctrl, opts, steps):
+    h = Handle(mesh, ctrl, **opts)
+    t = ctrl.dt
+    its = []
+    for _ in range(steps):
+        st = h.step(t, t if t <= 1.0 else 1.0).as_dict()
+        assert st["converged"]
+        its.append(st["ksp_its"])
+        t = t + ctrl.dt
+    s = h.get_solution()
+    h.close()
+    return s, its
+
+
+def _oracle(mesh, ctrl, opts, steps, threads):
+    fem = oracle.OracleFEM(mesh, ctrl, **bench.oracle_options(opts), threads=threads)
+    fem.solve(steps)
+    return fem.solution(), [st["gmres_its"] for st in fem.stats]
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _field_errors(a, b, ndof):
+    a = a.reshape(-1, ndof)
+    b = b.reshape(-1, ndof)
+    return {"velocity": _rel(a[:, :-1], b[:, :-1]), "pressure": _rel(a[:, -1], b[:, -1]), "all": _rel(a, b)}
+
+
+@pytest.mark.parametrize("steps", [10, pytest.param(50, marks=pytest.mark.slow)])
+def test_ldc3d_32_matches_oracle_with_bench_options(steps):
+    if steps > 10 and os.environ.get("CFDGPU_LONG_TESTS") != "1":
+        pytest.skip("all 50 steps run with CFDGPU_LONG_TESTS=1")
+    mesh, ctrl, opts = bench.make_case("ldc3d_32")
+    s_gpu, its_gpu = _gpu(mesh, ctrl, opts, steps)
+    nt = os.cpu_count() or 1
+    s_all, its_all = _oracle(mesh, ctrl, opts, steps, nt)
+    s_one, its_one = _oracle(mesh, ctrl, opts, steps, 1)
+    spread = _rel(s_one, s_all)
+    err = _rel(s_gpu, s_all)
+    rec = {"case": "ldc3d_32", "steps": steps, "solver": bench.solver_label(opts), "host_threads": nt,
+           "gpu_vs_oracle": _field_errors(s_gpu, s_all, mesh.ndof),
+           "oracle_1_vs_all_threads": _field_errors(s_one, s_all, mesh.ndof),
+           "its_gpu": its_gpu, "its_oracle": its_all}
+    path = os.environ.get("CFDGPU_PARITY_RECORD")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(rec) + "\n")
+    assert err <= max(1e-8, 2.0 * spread), rec
+    # same Newton structure; Krylov counts within max(2, 3 %) on every solve
+    assert [len(a) for a in its_gpu] == [len(b) for b in its_all]
+    assert all(abs(x - y) <= max(2, 0.03 * y) for a, b in zip(its_gpu, its_all) for x, y in zip(a, b)), rec

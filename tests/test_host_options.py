@@ -55,11 +55,11 @@ def test_gpu_keys():
     kw = solver_options_from_petsc({"-gpu_precision": "mixed", "-gpu_inner_restart": "100", "-gpu_inner_rtol": "1e-3",
                                     "-gpu_reuse_tangent": "0", "-gpu_refine_rtol": "1e-9",
                                     "-gpu_newton_rtol": "1e-2", "-gpu_guess": "Extrapolation",
-                                    "-gpu_formulation": "fully_implicit", "-gpu_ilu_chunk": "16",
+                                    "-gpu_formulation": "fully_implicit",
                                     "-pc_type": "pbjacobi"})
     assert kw["precision"] == "mixed" and kw["inner_restart"] == 100 and kw["inner_rtol"] == 1e-3
     assert kw["reuse_tangent"] is False and kw["refine_rtol"] == 1e-9 and kw["newton_rtol"] == 1e-2
-    assert kw["guess"] == "extrapolation" and kw["pc"] == "pbjacobi" and kw["ilu_chunk"] == 16
+    assert kw["guess"] == "extrapolation" and kw["pc"] == "pbjacobi"
     assert kw["formulation"] == "fully_implicit"
 
 
