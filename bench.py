@@ -71,8 +71,11 @@ def parse():
     p.add_argument("--solver", default=DEFAULT_SOLVER, choices=list(SOLVERS))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-variant", action="store_true",
+                   help="skip the mixed-precision + extrapolation-guess variant on the same time steps")
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                   help="mixed: FP32 tangent storage and FP32 inner GMRES(100) with FP64 refinement")
+                   help="mixed: FP64 flexible GMRES outer solves around FP32 BiCGStab inner solves with the FP32 "
+                        "preconditioner")
     p.add_argument("--method", default="plain", choices=["plain", "surrogate", "extrapolation", "batch", "kernels"],
                    help="surrogate / extrapolation: run the plain solve for --train-steps, then time the "
                         "following steps from that state with mixed precision and the learned (surrogate) or "
@@ -110,9 +113,19 @@ def make_case(name, precision="fp64", solver=DEFAULT_SOLVER):
     mesh, ctrl, _ = meshgen.case_hex(n, steps, mu=0.001, dt=0.1)
     opts = solver_options(name, solver)
     if precision == "mixed":
-        opts = {"restart": WORKLOADS[name][2], "rtol": 1e-10, "pc": "pbjacobi", "precision": "mixed",
-                "inner_restart": 100, "inner_rtol": 1e-4, "max_it": 40000}
+        opts = mixed_options(opts)
     return mesh, ctrl, opts
+
+
+def mixed_options(opts):
+    """Mixed-precision solver with the preconditioner of `opts`: FP64 flexible
+    GMRES(30) outer solves on the FP64 matrix to the step's Newton target,
+    preconditioned by 20 FP32 BiCGStab iterations (inner rtol 1e-2) on an FP32
+    copy with the FP32 form of the same preconditioner."""
+    o = {k: v for k, v in opts.items() if k in ("pc", "ilu_levels", "bjacobi_blocks")}
+    o.update(ksp="gmres", restart=30, rtol=1e-10, refine_rtol=1e-10, precision="mixed", inner_restart=20,
+             inner_rtol=1e-2, max_it=2000)
+    return o
 
 
 def oracle_options(opts):
@@ -143,8 +156,8 @@ def workload_config(name, mesh, opts, extra=None):
     cfg = {"workload": f"{name}: graded-cube lid-driven cavity, {n}^3 hex8 ({mesh.nElem} elements, "
                        f"{mesh.nNode} nodes, {mesh.nNode * 4} dofs), Re 1000, dt 0.1, gen-alpha rho_inf 0",
            "method": ("plain (reference-identical constant predictor), FP64" if opts.get("precision", "fp64") == "fp64"
-                      else "plain predictor, mixed precision: FP32 tangent + FP32 GMRES(100) cycles, FP64 refinement "
-                           "and FP64 Newton residual"),
+                      else "plain predictor, mixed precision: FP64 flexible GMRES outer solves, FP32 BiCGStab + FP32 "
+                           "preconditioner inner solves, FP64 Newton residual"),
            "solver": f"Newton to 1e-8 abs; {solver_label(opts)}",
            "l2": "flushed between timed steps (256 MiB write)"}
     if extra:
@@ -346,6 +359,12 @@ def run_ours(args, world, rank, local):
                 "kernels": {k: {"launches": v[0], "ms": round(v[1], 4),
                                 "gbs": (v[2] / (v[1] * 1e-3) / 1e9) if v[1] else None} for k, v in kinds.items()}}
 
+    # the mixed-precision + min-residual extrapolation-guess variant on the same
+    # time steps from the same state, with its field error against this run
+    variant = None
+    if not args.no_variant and args.precision == "fp64":
+        variant = run_variant(args, mesh, ctrl, opts, s0, p0, d0, t_start, s_final, total_ms, flush)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         st0 = stats[0]
@@ -366,8 +385,59 @@ def run_ours(args, world, rank, local):
             "krylov_iters": its,
             "all_converged": all(s["converged"] for s in stats),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks}
+            "mixed_guess_variant": variant, "clocks": clocks}
     return line
+
+
+def field_errors(a, b, ndof):
+    import numpy as np
+    a = a.reshape(-1, ndof)
+    b = b.reshape(-1, ndof)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    return {"all": rel(a, b), "velocity": rel(a[:, :-1], b[:, :-1]), "pressure": rel(a[:, -1], b[:, -1])}
+
+
+def run_variant(args, mesh, ctrl, opts, s0, p0, d0, t_start, s_plain, plain_ms, flush):
+    """Mixed precision (FP64 flexible GMRES around FP32 BiCGStab with the FP32
+    preconditioner) with the min-residual extrapolation initial guess, on the
+    timed steps of the plain run from the same state; device-timed like the
+    plain run."""
+    import statistics as stat
+    import torch
+    from cfdsfemmpi_b200 import Handle
+    kw = mixed_options(opts)
+    h = Handle(mesh, ctrl, guess="extrapolation", **kw)
+    h.set_solution(s0)
+    h.set_history(p0, d0)
+    stream = torch.cuda.ExternalStream(h.stream_ptr())
+    t = t_start
+    total, st = 0.0, []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st.append(h.step(t, t if t <= 1.0 else 1.0).as_dict())
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        t = t + ctrl.dt
+    sol = h.get_solution()
+    h.close()
+    return {"method": "mixed precision + min-residual extrapolation initial guess", "solver": solver_label(kw) +
+            f"; outer FGMRES({kw['restart']}) to max(1e-10 ||b||, 1e-9), inner {kw['inner_restart']} FP32 BiCGStab "
+            f"its (rtol {kw['inner_rtol']:g})",
+            "value": args.steps / (total * 1e-3), "unit": "steps/s", "ms_per_step": total / args.steps,
+            "speedup_vs_plain": plain_ms / total,
+            "outer_iters_per_step": stat.mean(sum(s["ksp_its"]) for s in st),
+            "newton_iters_per_step": stat.mean(s["newton_iters"] for s in st),
+            "guess_residual_ratio": stat.mean(s["guess_norm"] / s["plain_norm"] if s["plain_norm"] > 0 else 1.0
+                                              for s in st),
+            "all_converged": all(s["converged"] for s in st),
+            "final_residuals": [s["norms"][-1] for s in st],
+            "field_error_vs_plain_fp64": field_errors(sol, s_plain, mesh.ndof)}
 
 
 def _cpu_sample_once(fem, ctrl, state, t_start, nits):
@@ -509,7 +579,7 @@ def run_guess(args, world, rank, local):
     from cfdsfemmpi_b200.surrogate import train_guess
 
     torch.cuda.set_device(local)
-    mesh, ctrl, opts = make_case(args.workload)
+    mesh, ctrl, opts = make_case(args.workload, solver=args.solver)
     ramp_end = int(round(1.0 / ctrl.dt))          # the lid velocity ramps up to t = 1
     first = args.train_first or ramp_end + 2
     T0 = time.perf_counter()
@@ -527,7 +597,7 @@ def run_guess(args, world, rank, local):
     for name, (prec, guess) in GUESS_VARIANTS.items():
         kw = dict(opts)
         if prec == "mixed":
-            kw.update(precision="mixed", inner_restart=100, inner_rtol=1e-4, max_it=40000)
+            kw = mixed_options(opts)
             if args.newton_rtol > 0:
                 kw.update(newton_rtol=args.newton_rtol, newton_max_iter=30)
         if name == "reference_tight":
@@ -594,7 +664,7 @@ def run_guess(args, world, rank, local):
               if args.method == "surrogate" else
               "min-residual extrapolation initial guess (u_n + a (u_n - u_{n-1}), a minimising the affine "
               "iteration-0 residual)") + \
-        " + FP32 tangent/inner GMRES(100) with FP64 refinement and FP64 Newton residual"
+        " + mixed precision (FP64 flexible GMRES around FP32 BiCGStab with the FP32 preconditioner)"
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "impl": "ours", "method": head_name,
@@ -740,12 +810,12 @@ def run_batch(args, world, rank, local):
               "latency_ms": {"p50": float(np.percentile(lat_x, 50)), "p99": float(np.percentile(lat_x, 99))},
               "gmres_iters": int(its_x), "max_velocity_rel_diff_vs_constant_predictor": max(dvx)}
 
-    # the same batch in mixed precision (FP32 tangent + inner GMRES(100),
+    # the same batch in mixed precision (FP64 flexible GMRES around FP32 BiCGStab,
     # FP64 refinement and Newton residual), same steps and schedule rule
     mixed = None
     if not args.no_batch_mixed:
-        bm = Batch(pairs, **dict(BATCH_SOLVER, precision="mixed", inner_restart=100, inner_rtol=1e-4,
-                                 max_it=40000))
+        bm = Batch(pairs, **dict(BATCH_SOLVER, restart=30, precision="mixed", inner_restart=20, inner_rtol=1e-2,
+                                 max_it=2000))
         bm.set_schedule(0, 0, 0)
         for k in range(warm):
             bm.step(times(k))

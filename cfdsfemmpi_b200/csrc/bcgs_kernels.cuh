@@ -28,6 +28,7 @@ namespace cfdgpu {
 struct BcgsState {
   int its, reason, active, maxit;
   int tzero;                // (t, t) = 0 and (s, s) = 0: x += alpha p ends the solve
+  int skip;                 // inner solve of a flexible GMRES step whose cycle has ended: nothing runs
   double rtol, atol, dtol, rnorm0, ttol;
   double rho, rhoold, alpha, omega, omegaold, beta, dp;
   unsigned int counter;
@@ -46,9 +47,11 @@ __device__ __forceinline__ int bcgs_converged(BcgsState *s, int n_its, double rn
   return 0;
 }
 
-__global__ void bcgs_setup(BcgsState *st, int maxit, double rtol, double atol, double dtol)
+__global__ void bcgs_setup(BcgsState *st, int maxit, double rtol, double atol, double dtol,
+                           const GmresState *__restrict__ outer = nullptr, int j = 0)
 {
   if (threadIdx.x || blockIdx.x) return;
+  st->skip = (outer && (!outer->active || outer->it != j)) ? 1 : 0;
   st->its = 0; st->reason = 0; st->active = 0; st->maxit = maxit; st->tzero = 0;
   st->rtol = rtol; st->atol = atol; st->dtol = dtol; st->rnorm0 = 0.0; st->ttol = 0.0;
   st->rho = 0.0; st->rhoold = 1.0; st->alpha = 1.0; st->omega = 1.0; st->omegaold = 1.0; st->beta = 0.0;
@@ -63,6 +66,7 @@ __global__ void __launch_bounds__(RED_THREADS)
 bcgs_init(int64_t n, const VT *__restrict__ r, VT *__restrict__ rp, VT *__restrict__ p, VT *__restrict__ v,
           BcgsState *st, double *__restrict__ partial)
 {
+  if (st->skip) return;
   __shared__ double sh[RED_THREADS / 32];
   double s = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RED_THREADS) {

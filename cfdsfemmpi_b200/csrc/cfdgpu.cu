@@ -68,17 +68,20 @@ struct cfdgpu_handle {
   double *dinv = nullptr, *binv = nullptr;
   int m = 0;
   int64_t ldv = 0;     // Krylov vector stride (multiple of 32 entries, zero padded)
-  // mixed precision
+  // mixed precision: FP64 flexible GMRES outer solve on the FP64 matrix, FP32
+  // BiCGStab inner solves on an FP32 copy with an FP32 preconditioner
   bool mixed = false;
-  float *bsr32 = nullptr, *dinv32 = nullptr, *binv32 = nullptr, *V32 = nullptr, *b32 = nullptr;
-  double *r64 = nullptr, *d64 = nullptr;
-  int m32 = 0;
-  double inner_rtol = 1e-4, refine_rtol = 1e-6;
-  GmresState *gst32 = nullptr;
-  GmresArrays ga32{};
+  float *bsr32 = nullptr, *dinv32 = nullptr, *binv32 = nullptr, *b32 = nullptr;
+  float *fval32 = nullptr, *fdinv32 = nullptr, *ptmp32 = nullptr;
+  float *iR = nullptr, *iRP = nullptr, *iP = nullptr, *iV = nullptr, *iS = nullptr, *iT = nullptr;
+  BcgsState *ist = nullptr;
+  double *Zb = nullptr, *ones = nullptr;   // flexible GMRES: preconditioned directions, unit scales
+  int inner_its = 20;
+  double inner_rtol = 1e-2, refine_rtol = 1e-10;
   // Arnoldi chunks captured as CUDA graphs (per Krylov space, per chunk start)
   bool use_graphs = true;
-  std::vector<cudaGraphExec_t> graphs64, graphs32;
+  std::vector<cudaGraphExec_t> graphs64, graphs32;   // graphs32: flexible GMRES steps (mixed mode)
+  std::vector<int64_t> glaunch64, glaunch32;
   double *V = nullptr;
   GmresState *gst = nullptr;
   GmresArrays ga{};
@@ -370,16 +373,9 @@ static int launch_elements(cfdgpu_handle *h, const int32_t *elems, int nel, doub
   ElemParams P;
   P.rho = h->ctrl.rho; P.mu = h->ctrl.mu; P.af = h->td[2]; P.am = h->td[1]; P.acceFact = h->td[8];
   P.stab0 = h->ctrl.stab[0]; P.stab1 = h->ctrl.stab[1]; P.stab2 = h->ctrl.stab[2];
-  if (h->mixed && MODE != MODE_EXPORT) {
-    // FP64 arithmetic, FP32 storage of the tangent blocks
-    element_kernel<ET, double, float, MODE, LIFT, GROUPS, FORM><<<grid, GS * GROUPS, 0, h->stream>>>(
-        elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr32,
-        h->rhs, outK, outF, h->negjac);
-  } else {
-    element_kernel<ET, double, double, MODE, LIFT, GROUPS, FORM><<<grid, GS * GROUPS, 0, h->stream>>>(
-        elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
-        h->rhs, outK, outF, h->negjac);
-  }
+  element_kernel<ET, double, double, MODE, LIFT, GROUPS, FORM><<<grid, GS * GROUPS, 0, h->stream>>>(
+      elems, nel, h->conn, h->coords, h->prev, h->cur, h->dotCur, h->applied, h->fixmask, P, h->slot, h->bsr,
+      h->rhs, outK, outF, h->negjac);
   prof_end(h, pi);
   LAUNCHED(h);
   return check_launch(h, "element_kernel");
@@ -425,14 +421,21 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
   }
   if (want_K && !t.fixed_dofs.empty()) {
     const int nfix = (int)t.fixed_dofs.size();
-    if (h->mixed)
-      k_dirichlet_diag<float><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr32);
-    else
-      k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
+    k_dirichlet_diag<double><<<(nfix + 255) / 256, 256, 0, h->stream>>>(nfix, h->ndof, h->fixed_dofs, h->diag_slot, h->bsr);
     LAUNCHED(h);
     int rc = check_launch(h, "dirichlet_diag");
     if (rc) return rc;
+  }
+  if (want_K) {
     h->assembled_K = true;
+    if (h->mixed) {
+      // FP32 copy of the tangent for the inner solves
+      const int64_t cnt = h->topo.nnzb() * h->ndof * h->ndof;
+      k_round_to_f32<<<grid_for(cnt), 256, 0, h->stream>>>(cnt, h->bsr, h->bsr32);
+      LAUNCHED(h);
+      int rc = check_launch(h, "round_to_f32");
+      if (rc) return rc;
+    }
   }
 
 
@@ -461,6 +464,49 @@ static double trsv_bytes(cfdgpu_handle *h)
   // the vector in, intermediate (written and read) and out
   const double bb = (double)h->ndof * h->ndof * 8.0, V = 8.0 * h->n;
   return (double)h->ilu.nnzb() * (bb + 4.0) + (double)h->nNode * bb + 4.0 * V;
+}
+
+// numeric block ILU of the FP32 copy (mixed mode: FP64 arithmetic, FP32 factors)
+static int ilu_factor_run32(cfdgpu_handle *h)
+{
+  const int pi = prof_begin(h, CFDGPU_KIND_ILU, 0.5 * ilu_factor_bytes(h));
+  const int grid = ilu_grid(h->nNode);
+  if (h->ndof == 4)
+    ilu_factor<4, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr32, h->frow,
+                                                                    h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                    h->fval32, h->fdinv32, h->iflags, h->tctl);
+  else
+    ilu_factor<3, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr32, h->frow,
+                                                                    h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                    h->fval32, h->fdinv32, h->iflags, h->tctl);
+  prof_end(h, pi);
+  LAUNCHED(h);
+  return check_launch(h, "ilu_factor32");
+}
+
+// z = (L U)^-1 r with the FP32 factors on FP32 vectors
+static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresState *st, int j, const int *active)
+{
+  const int pi = prof_begin(h, CFDGPU_KIND_TRSV, 0.5 * trsv_bytes(h));
+  const int grid = ilu_grid(h->nNode);
+  if (h->ndof == 4) {
+    ilu_trsv<4, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, r, z, h->iflags, h->tctl, st, j,
+        active);
+    ilu_trsv<4, true, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, nullptr, z, h->iflags, h->tctl, st,
+        j, active);
+  } else {
+    ilu_trsv<3, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, r, z, h->iflags, h->tctl, st, j,
+        active);
+    ilu_trsv<3, true, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
+        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, nullptr, z, h->iflags, h->tctl, st,
+        j, active);
+  }
+  prof_end(h, pi);
+  h->launches += 2;
+  return check_launch(h, "ilu_solve32");
 }
 
 // numeric block ILU of the assembled FP64 matrix
@@ -527,7 +573,7 @@ static int build_pc(cfdgpu_handle *h)
 {
   const int pc = h->opts.pc_type;
   if (pc == CFDGPU_PC_NONE) return 0;
-  if (pc == CFDGPU_PC_BJACOBI_ILU) return ilu_factor_run(h);
+  if (pc == CFDGPU_PC_BJACOBI_ILU) return h->mixed ? ilu_factor_run32(h) : ilu_factor_run(h);
   const int g = (h->nNode + 127) / 128;
   if (h->mixed && h->ndof == 4) {
     build_jacobi<4, float, float><<<g, 128, 0, h->stream>>>(h->nNode, h->diag_slot, h->bsr32, h->dinv32, h->binv32, pc);
@@ -594,26 +640,34 @@ static int spmv_pc(cfdgpu_handle *h, int mode, const double *x, const double *b,
 }
 
 // y = M32^-1 (A32 x), FP32 vectors (mixed-precision inner solve)
-static int spmv32_pc(cfdgpu_handle *h, const float *x, float *y, const GmresState *st, int j, const double *xscale)
+static int spmv32_pc(cfdgpu_handle *h, const float *x, float *y, const GmresState *st, int j, const double *xscale,
+                     const int *active = nullptr)
 {
   const int pc = h->opts.pc_type;
+  if (pc == CFDGPU_PC_BJACOBI_ILU) {
+    h->opts.pc_type = CFDGPU_PC_NONE;
+    int rc = spmv32_pc(h, x, h->ptmp32, st, j, xscale, active);
+    h->opts.pc_type = CFDGPU_PC_BJACOBI_ILU;
+    if (rc) return rc;
+    return ilu_apply32(h, h->ptmp32, y, st, j, active);
+  }
   const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 0, 4, 4, pc));
   if (h->ndof == 4) {
     const int grid = (int)((h->nNode * 32LL + 255) / 256);
     if (pc == 0)
-      bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+      bsr4_spmv_f32<0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale, active);
     else if (pc == 1)
-      bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+      bsr4_spmv_f32<1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale, active);
     else
-      bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+      bsr4_spmv_f32<2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale, active);
   } else {
     const int grid = (int)((h->n + 255) / 256);
     if (pc == 0)
-      bsr_spmv_generic_f32<3, 0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+      bsr_spmv_generic_f32<3, 0><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale, active);
     else if (pc == 1)
-      bsr_spmv_generic_f32<3, 1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+      bsr_spmv_generic_f32<3, 1><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale, active);
     else
-      bsr_spmv_generic_f32<3, 2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale);
+      bsr_spmv_generic_f32<3, 2><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, h->dinv32, h->binv32, y, st, j, xscale, active);
   }
   prof_end(h, pi);
   LAUNCHED(h);
@@ -659,8 +713,11 @@ struct Krylov {
   int64_t ldv = 0;
   GmresState *st = nullptr;
   GmresArrays ga{};
+  double *Z = nullptr;   // flexible GMRES: x += sum_k y_k Z_k (with gaz.sigma = 1)
+  GmresArrays gaz{};
   std::vector<cudaGraphExec_t> &graphs;
-  explicit Krylov(std::vector<cudaGraphExec_t> &g) : graphs(g) {}
+  std::vector<int64_t> &graph_launches;   // kernel launches inside each cached graph
+  Krylov(std::vector<cudaGraphExec_t> &g, std::vector<int64_t> &gl) : graphs(g), graph_launches(gl) {}
 };
 
 // Restarted GMRES with PETSc semantics on a Krylov space.  The caller has
@@ -713,7 +770,10 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
       const int nk = std::min(m, j0 + CH) - j0;
       if (h->use_graphs && !h->prof) {
         std::vector<cudaGraphExec_t> &cache = K.graphs;
-        if (cache.size() < (size_t)((m + CH - 1) / CH)) cache.resize((m + CH - 1) / CH, nullptr);
+        if (cache.size() < (size_t)((m + CH - 1) / CH)) {
+          cache.resize((m + CH - 1) / CH, nullptr);
+          K.graph_launches.resize(cache.size(), 0);
+        }
         cudaGraphExec_t &ex = cache[j0 / CH];
         if (!ex) {
           cudaGraph_t g = nullptr;
@@ -725,13 +785,14 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
           if (ec != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(ec); return CFDGPU_ECUDA; }
           CK(cudaGraphInstantiate(&ex, g, 0));
           CK(cudaGraphDestroy(g));
+          K.graph_launches[j0 / CH] = h->launches - before + 2 * nk;
           h->launches = before;   // counted when the graph runs
         }
         CK(cudaGraphLaunch(ex, h->stream));
-        h->launches += 3 * nk;
+        h->launches += K.graph_launches[j0 / CH];
       } else {
         if ((rc = enqueue_chunk(j0))) return rc;
-        h->launches += 3 * nk;
+        h->launches += 2 * nk;
       }
       const int cidx = c % R;
       CK(cudaMemcpyAsync(&h->h_gst[cidx], st, sizeof(GmresState), cudaMemcpyDeviceToHost, h->stream));
@@ -745,7 +806,10 @@ static int gmres_run(cfdgpu_handle *h, Krylov<VT> &K, double *x, int max_it, dou
     }
     gmres_backsub<<<1, 1024, 0, h->stream>>>(st, K.ga);
     h->launches += 1;
-    gmres_update_x<VT><<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, V, ldv, st, K.ga, 1.0);
+    if (K.Z)
+      gmres_update_x<double><<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, K.Z, ldv, st, K.gaz, 1.0);
+    else
+      gmres_update_x<VT><<<vgrid, ORTHO_THREADS, 0, h->stream>>>(n, x, V, ldv, st, K.ga, 1.0);
     h->launches += 1;
     if ((rc = check_launch(h, "gmres_build_soln"))) return rc;
     GmresState *fin = h->h_gst + cfdgpu_handle::MAX_DEPTH + 1;
@@ -782,7 +846,7 @@ static int gmres(cfdgpu_handle *h, const double *b, double *x, int *its_out, int
 {
   int rc0 = pc_apply_vec(h, b, h->V);
   if (rc0) return rc0;
-  Krylov<double> K(h->graphs64);
+  Krylov<double> K(h->graphs64, h->glaunch64);
   K.V = h->V; K.m = h->m; K.ldv = h->ldv; K.st = h->gst; K.ga = h->ga;
   auto arn = [&](int j) {
     return spmv_pc(h, 0, h->V + (int64_t)j * h->ldv, nullptr, h->V + (int64_t)(j + 1) * h->ldv, h->gst, j, h->ga.sigma + j);
@@ -900,76 +964,88 @@ static int krylov_solve(cfdgpu_handle *h, const double *b, double *x, int *its, 
   return rc;
 }
 
-// Mixed precision linear solve (4x4 blocks): FP64 iterative refinement around
-// FP32 GMRES cycles.  x64 = 0, r64 = b; per pass: b32 = r64/||r64||, one FP32
-// GMRES(m_inner) cycle (FP32 matrix, FP32 Krylov basis, FP32 preconditioner;
-// FP64 dot products and Hessenberg) to the inner tolerance,
-// x64 += ||r64|| * d, r64 = b - A32 x64 accumulated in FP64.
-// Stops when ||r64|| <= max(refine_rtol*||b||, 0.1*T) or after max passes,
-// T the step's Newton stopping residual (newton_tol, or the relative target
-// when newton_rtol is set): the linear solve is not carried below it, and
-// the Newton loop's FP64 residual (element kernels in FP64) decides whether
-// the step has converged and corrects the FP32 rounding of the tangent.
-static int solve_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *passes_out,
-                       int *reason_out)
+// z32 = M32^-1 r32 (FP32 preconditioner of the inner solves)
+static int pc32_apply_vec(cfdgpu_handle *h, const float *r, float *z, const GmresState *st, int j)
+{
+  const int64_t n = h->n;
+  if (h->opts.pc_type == CFDGPU_PC_BJACOBI_ILU) return ilu_apply32(h, r, z, st, j, nullptr);
+  if (h->ndof == 4)
+    pc_apply<4, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, r, z);
+  else
+    pc_apply<3, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, r, z);
+  LAUNCHED(h);
+  return check_launch(h, "pc32_apply");
+}
+
+// Inner solve of flexible GMRES step j (mixed mode): z = (FP32 BiCGStab with
+// the FP32 preconditioner, at most inner_its iterations or inner_rtol) applied
+// to the normalised Arnoldi vector sigma_j V_j; z accumulates in FP64.  Every
+// kernel is skipped once the outer cycle has ended, so whole outer steps can
+// be enqueued (and captured) without host round trips.
+static int inner_bcgs32(cfdgpu_handle *h, const double *vj, const double *sigma_j, double *z, const GmresState *ost,
+                        int j)
 {
   const int64_t n = h->n;
   int rc;
-  CK(cudaMemsetAsync(x, 0, sizeof(double) * n, h->stream));
-  CK(cudaMemcpyAsync(h->r64, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
-  double bnorm = 0.0;
-  if ((rc = norm2(h, b, &bnorm))) return rc;
-  const double target = std::max(h->refine_rtol * bnorm, 0.1 * h->newton_target);
-  int total = 0, passes = 0, reason = 2;
-  double rn = bnorm;
-  Krylov<float> K(h->graphs32);
-  K.V = h->V32; K.m = h->m32; K.ldv = h->ldv; K.st = h->gst32; K.ga = h->ga32;
-  const int max_passes = 100;
-  while (rn > target && passes < max_passes && total < h->opts.max_it) {
-    // b32 = r64 / ||r64|| (the device norm lives in scalar[1])
-    if ((rc = norm2_dev(h, h->r64, h->scalar + 1))) return rc;
-    k_scale_to_f32<<<grid_for(n), 256, 0, h->stream>>>(n, h->r64, h->scalar + 1, h->b32);
-    if (h->ndof == 4)
-      pc_apply<4, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
-    else
-      pc_apply<3, float, float><<<grid_for(n, 256, 1 << 30), 256, 0, h->stream>>>(n, h->opts.pc_type, h->dinv32, h->binv32, h->b32, h->V32);
-    h->launches += 2;
-    if ((rc = check_launch(h, "mixed_prepare"))) return rc;
-    auto arn = [&](int j) {
-      return spmv32_pc(h, h->V32 + (int64_t)j * h->ldv, h->V32 + (int64_t)(j + 1) * h->ldv, h->gst32, j, h->ga32.sigma + j);
-    };
-    auto nores = [&]() { return 0; };
-    int its = 0, r = 0;
-    if ((rc = gmres_run<float>(h, K, h->d64, h->m32, h->inner_rtol, 1e-50, 1e4, true, arn, nores, &its, &r)))
-      return rc;
-    total += its;
-    if (r == -9) { reason = -9; break; }    // NaN/Inf in the inner solve
-    // x += ||r|| d ; r = b - A32 x (FP64 accumulation)
-    k_axpy_dev<<<grid_for(n), 256, 0, h->stream>>>(n, h->scalar + 1, h->d64, x);
-    LAUNCHED(h);
-    {
-      const int pi = prof_begin(h, CFDGPU_KIND_SPMV, spmv_bytes(h, 1, 8, 4, 0));
-      if (h->ndof == 4) {
-        const int grid = (int)((h->nNode * 32LL + 255) / 256);
-        bsr4_spmv<1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b, nullptr,
-                                                             nullptr, h->r64, nullptr, 0, nullptr);
-      } else {
-        const int grid = (int)((h->n + 255) / 256);
-        bsr_spmv_generic<3, 1, 0, float><<<grid, 256, 0, h->stream>>>(h->nNode, h->rowptr, h->colidx, h->bsr32, x, b,
-                                                                      nullptr, nullptr, h->r64, nullptr, 0, nullptr);
-      }
-      prof_end(h, pi);
-      LAUNCHED(h);
-      if ((rc = check_launch(h, "mixed_residual"))) return rc;
-    }
-    passes++;
-    if ((rc = norm2(h, h->r64, &rn))) return rc;
+  BcgsState *st = h->ist;
+  const int *act = &st->active;
+  k_scale_v_to_f32<<<grid_for(n), 256, 0, h->stream>>>(n, vj, sigma_j, h->b32, ost, j);
+  bcgs_setup<<<1, 1, 0, h->stream>>>(st, h->inner_its, h->inner_rtol, 1e-50, 1e30, ost, j);
+  h->launches += 2;
+  CK(cudaMemsetAsync(z, 0, sizeof(double) * n, h->stream));
+  if ((rc = pc32_apply_vec(h, h->b32, h->iR, ost, j))) return rc;
+  bcgs_init<float><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, h->iR, h->iRP, h->iP, h->iV, st, h->red_partial2);
+  LAUNCHED(h);
+  const int vgrid = grid_for(n);
+  for (int k = 0; k < h->inner_its; k++) {
+    bcgs_p<float><<<vgrid, 256, 0, h->stream>>>(n, h->iR, h->iV, h->iP, st);
+    if ((rc = spmv32_pc(h, h->iP, h->iV, nullptr, 0, nullptr, act))) return rc;
+    bcgs_alpha<float><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, h->iV, h->iRP, st, h->red_partial2);
+    bcgs_s<float><<<vgrid, 256, 0, h->stream>>>(n, h->iR, h->iV, h->iS, st);
+    if ((rc = spmv32_pc(h, h->iS, h->iT, nullptr, 0, nullptr, act))) return rc;
+    bcgs_omega<float><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, h->iS, h->iT, st, h->red_partial2);
+    bcgs_xr<float><<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, z, h->iP, h->iS, h->iT, h->iR, h->iRP, st,
+                                                             h->red_partial2);
+    h->launches += 5;
   }
-  if (rn > target) reason = (total >= h->opts.max_it) ? -3 : (reason < 0 ? reason : 0);
-  if (its_out) *its_out = total;
-  if (passes_out) *passes_out = passes;
-  if (reason_out) *reason_out = (rn <= target) ? 2 : reason;
-  return 0;
+  return check_launch(h, "inner_bcgs32");
+}
+
+// y = A x (mode 0) or b - A x (mode 1) with the FP64 matrix, no preconditioner
+static int spmv64_plain(cfdgpu_handle *h, int mode, const double *x, const double *b, double *y,
+                        const GmresState *st, int j)
+{
+  const int saved = h->opts.pc_type;
+  h->opts.pc_type = CFDGPU_PC_NONE;
+  const int rc = spmv_pc(h, mode, x, b, y, st, j, nullptr, nullptr);
+  h->opts.pc_type = saved;
+  return rc;
+}
+
+// Mixed precision linear solve: flexible GMRES (right preconditioning, FP64
+// basis, Hessenberg, Givens rotations and residual on the FP64 matrix) whose
+// preconditioner is the FP32 inner solve above, x0 = 0.  The residual
+// estimate is the true residual ||b - A x||; the solve stops at
+// max(refine_rtol ||b||, T/10), T the step's Newton stopping residual, so the
+// Newton loop's FP64 residual test (element kernels in FP64) decides whether
+// the step has converged.
+static int fgmres_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
+{
+  const int64_t n = h->n;
+  CK(cudaMemcpyAsync(h->V, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+  Krylov<double> K(h->graphs32, h->glaunch32);
+  K.V = h->V; K.m = h->m; K.ldv = h->ldv; K.st = h->gst; K.ga = h->ga;
+  K.Z = h->Zb;
+  K.gaz = h->ga;
+  K.gaz.sigma = h->ones;
+  auto arn = [&](int j) {
+    int rc = inner_bcgs32(h, h->V + (int64_t)j * h->ldv, h->ga.sigma + j, h->Zb + (int64_t)j * h->ldv, h->gst, j);
+    if (rc) return rc;
+    return spmv64_plain(h, 0, h->Zb + (int64_t)j * h->ldv, nullptr, h->V + (int64_t)(j + 1) * h->ldv, h->gst, j);
+  };
+  auto res = [&]() { return spmv64_plain(h, 1, x, b, h->V, nullptr, 0); };
+  return gmres_run<double>(h, K, x, h->opts.max_it, h->refine_rtol, 0.1 * h->newton_target, h->opts.dtol, false,
+                           arn, res, its_out, reason_out);
 }
 
 static int upload_td(cfdgpu_handle *h)
@@ -1099,14 +1175,8 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     h->err = "unknown preconditioner";
     return CFDGPU_EINVAL;
   }
-  if (h->opts.pc_type == CFDGPU_PC_BJACOBI_ILU) {
-    if (h->opts.precision != CFDGPU_PREC_FP64) {
-      h->err = "the block ILU preconditioner runs in FP64 precision mode";
-      return CFDGPU_EINVAL;
-    }
-  }
   if (h->opts.ksp_type != CFDGPU_KSP_GMRES && h->opts.precision != CFDGPU_PREC_FP64) {
-    h->err = "BiCGStab and preonly run in FP64 precision mode";
+    h->err = "mixed precision solves with flexible GMRES (ksp_type CFDGPU_KSP_GMRES) around FP32 BiCGStab";
     return CFDGPU_EINVAL;
   }
   if (h->ctrl.newton_max_iter <= 0) h->ctrl.newton_max_iter = 10;
@@ -1154,39 +1224,33 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   h->mixed = (h->opts.precision == CFDGPU_PREC_MIXED);
   // Krylov stride: a multiple of 512 entries, so every update CTA covers whole chunks
   h->ldv = (n + 511) / 512 * 512;
+  if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
+  CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
   if (h->mixed) {
-    // FP32 tangent and FP32 inner Krylov space; the FP64 matrix is not stored
-    h->m32 = (h->opts.inner_restart > 0) ? h->opts.inner_restart : 100;
-    if (h->m32 > 1000) { h->err = "inner restart > 1000 is not supported"; return CFDGPU_EINVAL; }
-    h->inner_rtol = (h->opts.inner_rtol > 0.0) ? h->opts.inner_rtol : 1e-4;
+    // FP32 copy of the tangent, FP32 preconditioner and FP32 inner BiCGStab
+    // vectors; FP64 outer flexible GMRES (V and Z bases)
+    h->inner_its = (h->opts.inner_restart > 0) ? h->opts.inner_restart : 20;
+    if (h->inner_its > 1000) { h->err = "inner iterations > 1000 are not supported"; return CFDGPU_EINVAL; }
+    h->inner_rtol = (h->opts.inner_rtol > 0.0) ? h->opts.inner_rtol : 1e-2;
     h->refine_rtol = (h->opts.refine_rtol > 0.0) ? h->opts.refine_rtol : 1e-10;
-    h->m = 1;   // FP64 basis kept only as scratch
     if ((rc = dalloc(h, &h->bsr32, (size_t)t.nnzb() * bb))) return rc;
     CK(cudaMemset(h->bsr32, 0, sizeof(float) * t.nnzb() * bb));
     if ((rc = dalloc(h, &h->dinv32, (size_t)n))) return rc;
     if ((rc = dalloc(h, &h->binv32, (size_t)h->nNode * bb))) return rc;
-    if ((rc = dalloc(h, &h->V32, (size_t)h->ldv * (h->m32 + 1)))) return rc;
-    CK(cudaMemset(h->V32, 0, sizeof(float) * h->ldv * (h->m32 + 1)));
-    if ((rc = dalloc(h, &h->b32, (size_t)h->ldv))) return rc;
-    CK(cudaMemset(h->b32, 0, sizeof(float) * h->ldv));
-    if ((rc = dalloc(h, &h->r64, (size_t)n))) return rc;
-    if ((rc = dalloc(h, &h->d64, (size_t)n))) return rc;
-    if ((rc = dalloc(h, &h->gst32, 1))) return rc;
-    CK(cudaMemset(h->gst32, 0, sizeof(GmresState)));
-    if ((rc = dalloc(h, &h->ga32.H, (size_t)(h->m32 + 1) * h->m32))) return rc;
-    if ((rc = dalloc(h, &h->ga32.sigma, (size_t)h->m32 + 1))) return rc;
-    if ((rc = dalloc(h, &h->ga32.cs, (size_t)h->m32))) return rc;
-    if ((rc = dalloc(h, &h->ga32.sn, (size_t)h->m32))) return rc;
-    if ((rc = dalloc(h, &h->ga32.grs, (size_t)h->m32 + 1))) return rc;
-    if ((rc = dalloc(h, &h->ga32.y, (size_t)h->m32))) return rc;
-    const int64_t nt32 = (h->ldv / 4 + ORTHO_THREADS - 1) / ORTHO_THREADS + h->ldv / 4 / MAXPY_SPAN + 1;
-    if ((rc = dalloc(h, &h->ga32.partial, (size_t)(h->m32 + 1) * std::max<int64_t>(nt32, RED_BLOCKS)))) return rc;
-    if ((rc = dalloc(h, &h->ga32.coef, (size_t)h->m32 + 1))) return rc;
-    if ((rc = dalloc(h, &h->ga32.kcount, (size_t)h->m32 / MDOT_KC + 2))) return rc;
-    CK(cudaMemset(h->ga32.kcount, 0, sizeof(unsigned int) * (h->m32 / MDOT_KC + 2)));
+    if ((rc = dalloc(h, &h->b32, (size_t)n))) return rc;
+    CK(cudaMemset(h->b32, 0, sizeof(float) * n));
+    float **iv[] = {&h->iR, &h->iRP, &h->iP, &h->iV, &h->iS, &h->iT, &h->ptmp32};
+    for (float **v : iv) {
+      if ((rc = dalloc(h, v, (size_t)n))) return rc;
+      CK(cudaMemset(*v, 0, sizeof(float) * n));
+    }
+    if ((rc = dalloc(h, &h->ist, 1))) return rc;
+    CK(cudaMemset(h->ist, 0, sizeof(BcgsState)));
+    if ((rc = dalloc(h, &h->Zb, (size_t)h->ldv * h->m))) return rc;
+    CK(cudaMemset(h->Zb, 0, sizeof(double) * h->ldv * h->m));
+    std::vector<double> ones(h->m + 1, 1.0);
+    if ((rc = upload(h, &h->ones, ones.data(), ones.size()))) return rc;
   } else {
-    if ((rc = dalloc(h, &h->bsr, (size_t)t.nnzb() * bb))) return rc;
-    CK(cudaMemset(h->bsr, 0, sizeof(double) * t.nnzb() * bb));
     if ((rc = dalloc(h, &h->dinv, (size_t)n))) return rc;
     if ((rc = dalloc(h, &h->binv, (size_t)h->nNode * bb))) return rc;
   }
@@ -1229,10 +1293,17 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = upload(h, &h->fumap, f.umap.data(), f.umap.size()))) return rc;
     if ((rc = upload(h, &h->florder, f.lorder.data(), f.lorder.size()))) return rc;
     if ((rc = upload(h, &h->fuorder, f.uorder.data(), f.uorder.size()))) return rc;
-    if ((rc = dalloc(h, &h->fval, (size_t)f.nnzb() * bb))) return rc;
-    CK(cudaMemset(h->fval, 0, sizeof(double) * f.nnzb() * bb));
-    if ((rc = dalloc(h, &h->fdinv, (size_t)h->nNode * bb))) return rc;
-    CK(cudaMemset(h->fdinv, 0, sizeof(double) * h->nNode * bb));
+    if (h->mixed) {
+      if ((rc = dalloc(h, &h->fval32, (size_t)f.nnzb() * bb))) return rc;
+      CK(cudaMemset(h->fval32, 0, sizeof(float) * f.nnzb() * bb));
+      if ((rc = dalloc(h, &h->fdinv32, (size_t)h->nNode * bb))) return rc;
+      CK(cudaMemset(h->fdinv32, 0, sizeof(float) * h->nNode * bb));
+    } else {
+      if ((rc = dalloc(h, &h->fval, (size_t)f.nnzb() * bb))) return rc;
+      CK(cudaMemset(h->fval, 0, sizeof(double) * f.nnzb() * bb));
+      if ((rc = dalloc(h, &h->fdinv, (size_t)h->nNode * bb))) return rc;
+      CK(cudaMemset(h->fdinv, 0, sizeof(double) * h->nNode * bb));
+    }
     if ((rc = dalloc(h, &h->iflags, (size_t)h->nNode))) return rc;
     CK(cudaMemset(h->iflags, 0, sizeof(unsigned int) * h->nNode));
     if ((rc = dalloc(h, &h->tctl, 1))) return rc;
@@ -1435,7 +1506,9 @@ int cfdgpu_step(cfdgpu_handle *h, double timeNow, double timeFact, cfdgpu_step_s
     if (want_K && (rc = build_pc(h))) return rc;
     int its = 0, reason = 0, passes = 0;
     if (h->mixed) {
-      if ((rc = solve_mixed(h, h->rhs, h->dx, &its, &passes, &reason))) return rc;
+      if ((rc = fgmres_mixed(h, h->rhs, h->dx, &its, &reason))) return rc;
+      if ((rc = ilu_check(h))) return rc;
+      passes = its;
     } else {
       if ((rc = krylov_solve(h, h->rhs, h->dx, &its, &reason))) return rc;
     }
@@ -1609,7 +1682,6 @@ int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int
 int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double *rhs)
 {
   if (!h) return CFDGPU_EINVAL;
-  if (h->mixed && bsr_vals) { h->err = "the FP64 matrix is not stored in mixed precision"; return CFDGPU_EINVAL; }
 
   if (!h->td_set) upload_td(h);
   int rc = assemble(h, iter, true);
@@ -1644,6 +1716,7 @@ int cfdgpu_ilu_export(cfdgpu_handle *h, int64_t *nnzb, int32_t *rowptr, int32_t 
 {
   if (!h) return CFDGPU_EINVAL;
   if (h->opts.pc_type != CFDGPU_PC_BJACOBI_ILU) { h->err = "the handle has no ILU preconditioner"; return CFDGPU_EINVAL; }
+  if (h->mixed && (vals || dinv)) { h->err = "mixed precision keeps FP32 factors"; return CFDGPU_EINVAL; }
   const IluPattern &f = h->ilu;
   if (nnzb) *nnzb = f.nnzb();
   auto cp = [](int32_t *dst, const std::vector<int32_t> &v) { if (dst && !v.empty()) memcpy(dst, v.data(), v.size() * 4); };
@@ -1676,7 +1749,6 @@ int cfdgpu_pc_apply_export(cfdgpu_handle *h, const double *r, double *z)
 int cfdgpu_true_residual(cfdgpu_handle *h, const double *x, const double *b, double *norm)
 {
   if (!h || !x || !b || !norm) return CFDGPU_EINVAL;
-  if (h->mixed) { h->err = "cfdgpu_true_residual uses the FP64 matrix"; return CFDGPU_EINVAL; }
 
   if (!h->assembled_K) { h->err = "assemble the matrix first"; return CFDGPU_EINVAL; }
   // x -> dx, b -> rhs, r = b - A x -> applied-free scratch (the Krylov vector V_0)

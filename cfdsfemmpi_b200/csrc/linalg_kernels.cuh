@@ -164,9 +164,10 @@ __global__ void __launch_bounds__(256)
 bsr4_spmv_f32(int nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
               const float *__restrict__ val, const float *__restrict__ x, const float *__restrict__ dinv,
               const float *__restrict__ binv, float *__restrict__ y, const GmresState *__restrict__ st, int j,
-              const double *__restrict__ xscale)
+              const double *__restrict__ xscale, const int *__restrict__ active = nullptr)
 {
   if (st && (!st->active || st->it != j)) return;
+  if (active && !active[0]) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nrows) return;
@@ -254,9 +255,10 @@ __global__ void bsr_spmv_generic_f32(int nrows, const int32_t *__restrict__ rowp
                                      const float *__restrict__ val, const float *__restrict__ x,
                                      const float *__restrict__ dinv, const float *__restrict__ binv,
                                      float *__restrict__ y, const GmresState *__restrict__ st, int j,
-                                     const double *__restrict__ xscale)
+                                     const double *__restrict__ xscale, const int *__restrict__ active = nullptr)
 {
   if (st && (!st->active || st->it != j)) return;
+  if (active && !active[0]) return;
   const float xs = xscale ? (float)xscale[0] : 1.f;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t node = t / NB;
@@ -784,6 +786,24 @@ gmres_update_x(int64_t n, double *__restrict__ x, const VT *__restrict__ V, int6
     for (int k = 0; k < it; k++) s = fma(yk[k], (double)V[(int64_t)k * ldv + i], s);
     x[i] += scale * s;
   }
+}
+
+// FP32 copy of an FP64 array of any length
+__global__ void k_round_to_f32(int64_t n, const double *__restrict__ a, float *__restrict__ b)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// b32 = sigma * v (FP32): the normalised Arnoldi vector of a flexible GMRES
+// step, the right-hand side of its inner solve; skipped once the cycle ended
+__global__ void k_scale_v_to_f32(int64_t n, const double *__restrict__ v, const double *__restrict__ sigma,
+                                 float *__restrict__ b32, const GmresState *__restrict__ st, int j)
+{
+  if (st && (!st->active || st->it != j)) return;
+  const double s = sigma[0];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b32[i] = (float)(s * v[i]);
 }
 
 // mixed precision helpers: b32 = r64 * s (FP32), x64 += a * d64

@@ -63,7 +63,9 @@ extern "C" {
 
 /* precision modes */
 #define CFDGPU_PREC_FP64 0      /* FP64 element kernels, matrix and Krylov solve */
-#define CFDGPU_PREC_MIXED 1     /* FP32 tangent storage + FP32 inner GMRES, FP64 residual/refinement */
+#define CFDGPU_PREC_MIXED 1     /* FP64 flexible GMRES (FP64 matrix, basis, Hessenberg, residual) whose
+                                   preconditioner is an FP32 BiCGStab inner solve on an FP32 copy of the
+                                   tangent with the FP32 form of pc_type */
 
 /* Mesh: borrowed host arrays, copied at create (StabFEM::readInputData,
  * StabFEM.cpp:80-264).  conn is 0-based, nElem*npElem; DBC entries are
@@ -102,11 +104,11 @@ typedef struct cfdgpu_solver_opts {
   int max_it;
   int pc_type;
   int precision;            /* CFDGPU_PREC_* */
-  int inner_restart;        /* mixed mode: FP32 inner GMRES restart (0: 100) */
-  double inner_rtol;        /* mixed mode: inner relative tolerance per refinement pass (0: 1e-4) */
+  int inner_restart;        /* mixed mode: FP32 BiCGStab iterations per outer flexible-GMRES step (0: 20) */
+  double inner_rtol;        /* mixed mode: inner relative tolerance of those iterations (0: 1e-2) */
   int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
-  double refine_rtol;       /* mixed mode: refinement target ||b - A32 x|| <= max(refine_rtol ||b||, T/10), T the
-                               step's Newton target below (0: 1e-10) */
+  double refine_rtol;       /* mixed mode: outer target ||b - A x|| <= max(refine_rtol ||b||, T/10) on the FP64
+                               matrix, T the step's Newton target below (0: 1e-10); restart = outer restart */
   double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0||, F_0 the iteration-0
                                residual of the constant predictor (0: off, the reference's test only) */
   int formulation;          /* CFDGPU_FORM_*: element routine (0: the reference's active semi-implicit one) */
@@ -129,7 +131,7 @@ typedef struct cfdgpu_step_stats {
   double norms[CFDGPU_MAX_NEWTON];      /* residual 2-norm per Newton iteration */
   int ksp_its[CFDGPU_MAX_NEWTON];       /* Krylov iterations per solve */
   int ksp_reason[CFDGPU_MAX_NEWTON];    /* PETSc-style KSPConvergedReason per solve */
-  int refinements[CFDGPU_MAX_NEWTON];   /* mixed mode: outer refinement passes per solve */
+  int refinements[CFDGPU_MAX_NEWTON];   /* mixed mode: outer flexible-GMRES iterations per solve */
   double ms_assembly, ms_solver, ms_total;
   int guess_used;                       /* 1: the combined initial guess was kept */
   double guess_norm, plain_norm;        /* iteration-0 residual norms of both guesses (when a guess mode is set) */
