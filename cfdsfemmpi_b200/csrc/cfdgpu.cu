@@ -122,6 +122,8 @@ struct cfdgpu_handle {
   unsigned int *iflags = nullptr;
   TriCtl *tctl = nullptr, *h_tctl = nullptr;
   double *ptmp = nullptr;          // A x before the triangular solves
+  double *ybuf = nullptr;          // intermediate vector of the triangular solves (sentinel between solves)
+  float *ybuf32 = nullptr;
   // BiCGStab (ksp_type CFDGPU_KSP_BCGS)
   BcgsState *bst = nullptr, *h_bst = nullptr;
   double *bR = nullptr, *bRP = nullptr, *bP = nullptr, *bV = nullptr, *bS = nullptr, *bT = nullptr;
@@ -487,23 +489,16 @@ static int ilu_factor_run32(cfdgpu_handle *h)
 // z = (L U)^-1 r with the FP32 factors on FP32 vectors
 static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresState *st, int j, const int *active)
 {
+  if ((const void *)r == (const void *)z) { h->err = "ILU apply: input and output overlap"; return CFDGPU_EINVAL; }
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, 0.5 * trsv_bytes(h));
   const int grid = ilu_grid(h->nNode);
-  if (h->ndof == 4) {
-    ilu_trsv<4, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, r, z, h->iflags, h->tctl, st, j,
-        active);
-    ilu_trsv<4, true, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, nullptr, z, h->iflags, h->tctl, st,
-        j, active);
-  } else {
-    ilu_trsv<3, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, r, z, h->iflags, h->tctl, st, j,
-        active);
-    ilu_trsv<3, true, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, nullptr, z, h->iflags, h->tctl, st,
-        j, active);
-  }
+#define TRSV32(NB)                                                                                              \
+  ilu_trsv<NB, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->florder, h->frow, h->fcol, \
+      h->fdiag, h->fval32, h->fdinv32, r, h->ybuf32, z, h->tctl, st, j, active);                               \
+  ilu_trsv<NB, true, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->fuorder, h->frow, h->fcol,  \
+      h->fdiag, h->fval32, h->fdinv32, nullptr, h->ybuf32, z, h->tctl, st, j, active)
+  if (h->ndof == 4) { TRSV32(4); } else { TRSV32(3); }
+#undef TRSV32
   prof_end(h, pi);
   h->launches += 2;
   return check_launch(h, "ilu_solve32");
@@ -527,24 +522,19 @@ static int ilu_factor_run(cfdgpu_handle *h)
   return check_launch(h, "ilu_factor");
 }
 
-// z = (L U)^-1 r: lower solve r -> z, upper solve in place on z
+// z = (L U)^-1 r: lower solve r -> y (the handle's buffer), upper solve y -> z
 static int ilu_apply(cfdgpu_handle *h, const double *r, double *z, const GmresState *st, int j, const int *active)
 {
+  if ((const void *)r == (const void *)z) { h->err = "ILU apply: input and output overlap"; return CFDGPU_EINVAL; }
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, trsv_bytes(h));
   const int grid = ilu_grid(h->nNode);
-  if (h->ndof == 4) {
-    ilu_trsv<4, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, r, z, h->iflags, h->tctl, st, j, active);
-    ilu_trsv<4, true, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, nullptr, z, h->iflags, h->tctl, st, j,
-        active);
-  } else {
-    ilu_trsv<3, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->florder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, r, z, h->iflags, h->tctl, st, j, active);
-    ilu_trsv<3, true, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(
-        h->nNode, h->fuorder, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, nullptr, z, h->iflags, h->tctl, st, j,
-        active);
-  }
+#define TRSV64(NB)                                                                                                \
+  ilu_trsv<NB, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->florder, h->frow, h->fcol, \
+      h->fdiag, h->fval, h->fdinv, r, h->ybuf, z, h->tctl, st, j, active);                                         \
+  ilu_trsv<NB, true, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->fuorder, h->frow, h->fcol,  \
+      h->fdiag, h->fval, h->fdinv, nullptr, h->ybuf, z, h->tctl, st, j, active)
+  if (h->ndof == 4) { TRSV64(4); } else { TRSV64(3); }
+#undef TRSV64
   prof_end(h, pi);
   h->launches += 2;
   return check_launch(h, "ilu_solve");
@@ -560,6 +550,10 @@ static int ilu_check(cfdgpu_handle *h)
   const TriCtl c = *h->h_tctl;
   if (c.error == 0) return 0;
   CK(cudaMemsetAsync(&h->tctl->error, 0, sizeof(unsigned int), h->stream));
+  // a solve that stopped early leaves rows of the intermediate vector set:
+  // restore the sentinel before the next solve
+  if (h->ybuf) fill_sentinel_f64<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, h->ybuf);
+  if (h->ybuf32) fill_sentinel_f32<<<grid_for(h->n), 256, 0, h->stream>>>(h->n, h->ybuf32);
   if (c.error == ILU_ERR_ZERO_PIVOT) {
     h->err = "Zero pivot in the ILU factorisation (singular diagonal block at node " +
              std::to_string(c.zero_pivot_row) + ")";
@@ -1310,6 +1304,14 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     CK(cudaMemset(h->tctl, 0, sizeof(TriCtl)));
     if ((rc = dalloc(h, &h->ptmp, (size_t)n))) return rc;
     CK(cudaMemset(h->ptmp, 0, sizeof(double) * n));
+    if (h->mixed) {
+      if ((rc = dalloc(h, &h->ybuf32, (size_t)n))) return rc;
+      fill_sentinel_f32<<<grid_for(n), 256, 0, h->stream>>>(n, h->ybuf32);
+    } else {
+      if ((rc = dalloc(h, &h->ybuf, (size_t)n))) return rc;
+      fill_sentinel_f64<<<grid_for(n), 256, 0, h->stream>>>(n, h->ybuf);
+    }
+    CK(cudaStreamSynchronize(h->stream));
     CK(cudaMallocHost(&h->h_tctl, sizeof(TriCtl)));
   }
   if (h->opts.ksp_type == CFDGPU_KSP_BCGS) {

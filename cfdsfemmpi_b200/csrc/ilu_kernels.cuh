@@ -261,77 +261,152 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
 
 // ---------------------------------------------------------------------------
 // Triangular solves z = (L U)^-1 r, one warp per row, rows in level order
-// (lorder for the lower solve, uorder for the upper solve).  The lanes poll
-// the row's dependencies (one flag per row), accumulate the off-diagonal
-// products (32 / NB^2 blocks per warp step, fixed order), and lane 0 stores
-// the row's NB values and then its flag with a release store.
+// (lorder for the lower solve, uorder for the upper solve).
 //
-// Lower:  y_i = r_i - sum_{p<i} L_ip y_p              (in place over r allowed)
-// Upper:  z_i = U_ii^-1 (y_i - sum_{p>i} U_ip z_p)   (in place over y allowed)
+// The values are their own ready flags: the intermediate vector y and the
+// output z hold a signalling-NaN sentinel (a bit pattern no arithmetic
+// produces) until their row is written, so a row whose inputs are not ready
+// polls the input values themselves (relaxed loads with back-off) and needs
+// no separate flag, fence or second round trip.  The lower solve writes y_i
+// and resets z_i to the sentinel for the upper solve; the upper solve reads
+// y_i, writes z_i and resets y_i to the sentinel for the next lower solve.
+// y is the handle's own buffer (sentinel-filled at creation); r and z must
+// not overlap.
+//
+// Lower:  y_i = r_i - sum_{p<i} L_ip y_p
+// Upper:  z_i = U_ii^-1 (y_i - sum_{p>i} U_ip z_p)
 // st/j: inside a GMRES chunk the launch is skipped once the cycle has ended;
 // active: inside a BiCGStab chunk, once the solve has ended.
+template <typename VT> struct Sentinel;
+template <> struct Sentinel<double> {
+  using U = unsigned long long;
+  static constexpr U bits = 0x7FF4C0FFEE15BAD1ull;   // signalling NaN
+  static __device__ __forceinline__ U load(const double *p)
+  {
+    U v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+  }
+  static __device__ __forceinline__ void store(double *p, double x)
+  {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(x) : "memory");
+  }
+  static __device__ __forceinline__ double value(U v) { return __longlong_as_double((long long)v); }
+  static __device__ __forceinline__ double sentinel() { return __longlong_as_double((long long)bits); }
+};
+template <> struct Sentinel<float> {
+  using U = unsigned int;
+  static constexpr U bits = 0x7FA0C0DEu;               // signalling NaN
+  static __device__ __forceinline__ U load(const float *p)
+  {
+    U v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+  }
+  static __device__ __forceinline__ void store(float *p, float x)
+  {
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(x) : "memory");
+  }
+  static __device__ __forceinline__ float value(U v) { return __uint_as_float(v); }
+  static __device__ __forceinline__ float sentinel() { return __uint_as_float(bits); }
+};
+
+// value at p once it is no longer the sentinel (bounded wait)
+template <typename VT>
+__device__ __forceinline__ double wait_value(const VT *p, typename Sentinel<VT>::U v, TriCtl *ctl)
+{
+  using S = Sentinel<VT>;
+  if (v != S::bits) return (double)S::value(v);
+  unsigned int ns = 32;
+  for (int it = 0; it < ILU_SPIN_LIMIT; it++) {
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+    v = S::load(p);
+    if (v != S::bits) return (double)S::value(v);
+    if (*(volatile unsigned int *)&ctl->error) break;
+  }
+  atomicCAS(&ctl->error, 0u, ILU_ERR_TIMEOUT);
+  return 0.0;
+}
+
+__global__ void fill_sentinel_f64(int64_t n, double *y)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = Sentinel<double>::sentinel();
+}
+
+__global__ void fill_sentinel_f32(int64_t n, float *y)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = Sentinel<float>::sentinel();
+}
+
+constexpr int TRSV_BATCH = 4;   // input loads in flight per lane
+
 template <int NB, bool UPPER, typename FT, typename VT>
 __global__ void __launch_bounds__(ILU_THREADS)
 ilu_trsv(int n, const int32_t *__restrict__ order, const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol,
          const int32_t *__restrict__ fdiag, const FT *__restrict__ fval, const FT *__restrict__ fdinv, const VT *r,
-         VT *y, unsigned int *flags, TriCtl *ctl, const GmresState *__restrict__ st, int j,
-         const int *__restrict__ active)
+         VT *y, VT *z, TriCtl *ctl, const GmresState *__restrict__ st, int j, const int *__restrict__ active)
 {
   if (st && (!st->active || st->it != j)) return;
   if (active && !active[0]) return;
+  using S = Sentinel<VT>;
   constexpr int BB = NB * NB;
   constexpr int G = 32 / BB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   __shared__ double red[ILU_WARPS][32];
+  __shared__ double sv[ILU_WARPS][NB];
   const unsigned int epoch = *(volatile unsigned int *)&ctl->epoch;
-  const unsigned int target = epoch + 1u;
   const int g = lane / BB, e = lane % BB, ec = e % NB;
+  // the vector the off-diagonal products read: y (lower) or z (upper)
+  const VT *src = UPPER ? z : y;
   while (true) {
     const int tk = draw_ticket(ctl, lane);
     if (tk >= n) break;
     const int i = order[tk];
     const int q0 = UPPER ? fdiag[i] + 1 : fptr[i];
     const int q1 = UPPER ? fptr[i + 1] : fdiag[i];
-    for (int q = q0 + lane; q < q1; q += 32) wait_flag(flags + fcol[q], target, ctl);
-    __syncwarp();
-    fence_acq_rel_gpu();
     double acc = 0.0;
-    for (int qb = q0; qb < q1; qb += G) {
-      const int q = qb + g;
-      if (g < G && q < q1) {
-        const int p = fcol[q];
-        acc = fma((double)fval[(int64_t)q * BB + e], ld_cg(y + (int64_t)p * NB + ec), acc);
+    for (int qb = q0; qb < q1; qb += G * TRSV_BATCH) {
+      typename S::U v[TRSV_BATCH];
+      int p[TRSV_BATCH];
+      double a[TRSV_BATCH];
+#pragma unroll
+      for (int k = 0; k < TRSV_BATCH; k++) {
+        const int q = qb + k * G + g;
+        const bool ok = (g < G && q < q1);
+        p[k] = ok ? fcol[q] : -1;
+        a[k] = ok ? (double)fval[(int64_t)q * BB + e] : 0.0;
       }
+#pragma unroll
+      for (int k = 0; k < TRSV_BATCH; k++) v[k] = (p[k] >= 0) ? S::load(src + (int64_t)p[k] * NB + ec) : 0;
+#pragma unroll
+      for (int k = 0; k < TRSV_BATCH; k++)
+        if (p[k] >= 0) acc = fma(a[k], wait_value<VT>(src + (int64_t)p[k] * NB + ec, v[k], ctl), acc);
     }
     red[w][lane] = acc;
     __syncwarp();
-    double s = 0.0;
     if (lane < NB) {
-      s = UPPER ? ld_cg(y + (int64_t)i * NB + lane) : (double)r[(int64_t)i * NB + lane];
+      double s = UPPER ? (double)y[(int64_t)i * NB + lane] : (double)r[(int64_t)i * NB + lane];
 #pragma unroll
       for (int gg = 0; gg < G; gg++)
 #pragma unroll
         for (int c = 0; c < NB; c++) s -= red[w][gg * BB + lane * NB + c];
+      sv[w][lane] = s;
     }
-    if (UPPER) {
-      // z_i = U_ii^-1 s: lane a takes row a of the inverse
-      double sv[NB];
-#pragma unroll
-      for (int c = 0; c < NB; c++) sv[c] = __shfl_sync(0xffffffffu, s, c);
-      if (lane < NB) {
+    __syncwarp();
+    if (lane < NB) {
+      if (UPPER) {
         double v = 0.0;
 #pragma unroll
-        for (int c = 0; c < NB; c++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + c], sv[c], v);
-        s = v;
+        for (int c = 0; c < NB; c++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + c], sv[w][c], v);
+        S::store(z + (int64_t)i * NB + lane, (VT)v);
+        y[(int64_t)i * NB + lane] = S::sentinel();
+      } else {
+        z[(int64_t)i * NB + lane] = S::sentinel();
+        S::store(y + (int64_t)i * NB + lane, (VT)sv[w][lane]);
       }
-    }
-    double out[NB];
-#pragma unroll
-    for (int c = 0; c < NB; c++) out[c] = __shfl_sync(0xffffffffu, s, c);
-    if (lane == 0) {
-#pragma unroll
-      for (int c = 0; c < NB; c++) y[(int64_t)i * NB + c] = (VT)out[c];
-      st_release_u32(flags + i, target);
     }
     __syncwarp();
   }
