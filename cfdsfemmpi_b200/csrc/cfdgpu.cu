@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -445,11 +446,12 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
 }
 
 // Persistent grid of the sync-free ILU kernels: enough warps for `tasks`
-// rows, at most 4 CTAs of 8 warps per SM.
+// rows, at most g_ilu_ctas CTAs of 8 warps.
+static int g_ilu_ctas = 148 * 4;
 static inline int ilu_grid(int64_t tasks)
 {
   const int64_t ctas = (tasks + ILU_WARPS - 1) / ILU_WARPS;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(ctas, 148 * 4));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(ctas, g_ilu_ctas));
 }
 
 static double ilu_factor_bytes(cfdgpu_handle *h)
@@ -1153,6 +1155,7 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   h->n = (int64_t)h->nNode * h->ndof;
   h->ctrl = *ctrl;
   h->opts = *opts;
+  if (const char *e = getenv("CFDGPU_ILU_CTAS")) g_ilu_ctas = std::max(1, atoi(e));
   if (h->opts.restart <= 0) h->opts.restart = 30;
   if (h->opts.restart > 1000) { h->err = "restart > 1000 is not supported"; return CFDGPU_EINVAL; }
   if (h->opts.max_it <= 0) h->opts.max_it = 10000;

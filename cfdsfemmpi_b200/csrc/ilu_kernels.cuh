@@ -367,15 +367,20 @@ ilu_trsv(int n, const int32_t *__restrict__ order, const int32_t *__restrict__ f
     const int i = order[tk];
     const int q0 = UPPER ? fdiag[i] + 1 : fptr[i];
     const int q1 = UPPER ? fptr[i + 1] : fdiag[i];
+    // visit the row's blocks so that the nearest column (i-1 below the
+    // diagonal, i+1 above it: the input finished last) comes last, and the
+    // other products accumulate while it is still being computed
     double acc = 0.0;
-    for (int qb = q0; qb < q1; qb += G * TRSV_BATCH) {
+    const int nq = q1 - q0;
+    for (int qb = 0; qb < nq; qb += G * TRSV_BATCH) {
       typename S::U v[TRSV_BATCH];
       int p[TRSV_BATCH];
       double a[TRSV_BATCH];
 #pragma unroll
       for (int k = 0; k < TRSV_BATCH; k++) {
-        const int q = qb + k * G + g;
-        const bool ok = (g < G && q < q1);
+        const int qq = qb + k * G + g;
+        const bool ok = (g < G && qq < nq);
+        const int q = UPPER ? q1 - 1 - qq : q0 + qq;
         p[k] = ok ? fcol[q] : -1;
         a[k] = ok ? (double)fval[(int64_t)q * BB + e] : 0.0;
       }
