@@ -57,7 +57,7 @@ class SolverOpts(ctypes.Structure):
                 ("precision", ctypes.c_int), ("inner_restart", ctypes.c_int), ("inner_rtol", ctypes.c_double),
                 ("reuse_tangent", ctypes.c_int), ("refine_rtol", ctypes.c_double), ("newton_rtol", ctypes.c_double),
                 ("formulation", ctypes.c_int), ("ksp_type", ctypes.c_int), ("ilu_levels", ctypes.c_int),
-                ("bjacobi_blocks", ctypes.c_int)]
+                ("bjacobi_blocks", ctypes.c_int), ("refine_atol", ctypes.c_double)]
 
 
 class StepStats(ctypes.Structure):
@@ -188,13 +188,13 @@ def _mesh_struct(mesh):
 def _control_opts(ctrl, restart=50, rtol=1e-10, atol=1e-50, dtol=1e4, max_it=10000, pc="jacobi", precision="fp64",
                   inner_restart=0, inner_rtol=1e-4, reuse_tangent=True, newton_tol=1e-8, newton_max_iter=10,
                   refine_rtol=1e-10, newton_rtol=0.0, formulation="semi_implicit", ksp="gmres", ilu_levels=0,
-                  bjacobi_blocks=1):
+                  bjacobi_blocks=1, refine_atol=0.0):
     """(Control, SolverOpts) structs from an io.Control and solver keywords."""
     c = Control(ctrl.rho, ctrl.mu, (ctypes.c_double * 3)(*ctrl.bodyforce), (ctypes.c_double * 3)(*ctrl.stab),
                 ctrl.tis, ctrl.rhoInf, ctrl.dt, newton_tol, newton_max_iter)
     o = SolverOpts(restart, rtol, atol, dtol, max_it, PC[pc], PREC[precision], inner_restart, inner_rtol,
                    1 if reuse_tangent else 0, refine_rtol, newton_rtol, FORM[formulation], KSP[ksp], ilu_levels,
-                   bjacobi_blocks)
+                   bjacobi_blocks, refine_atol)
     return c, o
 
 
@@ -230,7 +230,7 @@ class Handle:
                  inner_rtol: float = 1e-4, reuse_tangent: bool = True, newton_tol: float = 1e-8,
                  newton_max_iter: int = 10, refine_rtol: float = 1e-10, newton_rtol: float = 0.0,
                  guess: str = "constant", formulation: str = "semi_implicit", ksp: str = "gmres",
-                 ilu_levels: int = 0, bjacobi_blocks: int = 1):
+                 ilu_levels: int = 0, bjacobi_blocks: int = 1, refine_atol: float = 0.0):
         L = load()
         self._L = L
         self.h = ctypes.c_void_p()
@@ -241,7 +241,7 @@ class Handle:
                              precision=precision, inner_restart=inner_restart, inner_rtol=inner_rtol,
                              reuse_tangent=reuse_tangent, newton_tol=newton_tol, newton_max_iter=newton_max_iter,
                              refine_rtol=refine_rtol, newton_rtol=newton_rtol, formulation=formulation, ksp=ksp,
-                             ilu_levels=ilu_levels, bjacobi_blocks=bjacobi_blocks)
+                             ilu_levels=ilu_levels, bjacobi_blocks=bjacobi_blocks, refine_atol=refine_atol)
         rc = L.cfdgpu_create(ctypes.byref(m), ctypes.byref(c), ctypes.byref(o), ctypes.byref(self.h))
         if rc != 0:
             msg = L.cfdgpu_last_error(self.h).decode() if self.h else "create failed"

@@ -446,12 +446,13 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
 }
 
 // Persistent grid of the sync-free ILU kernels: enough warps for `tasks`
-// rows, at most g_ilu_ctas CTAs of 8 warps.
-static int g_ilu_ctas = 148 * 4;
+// rows, at most 2 CTAs of 8 warps per SM.  More warps in flight only add
+// polling traffic: on the 115^3 cavity the triangular-solve pair takes 5.4 ms
+// with 2 CTAs per SM against 9.5 ms with 4 and 14 ms with 8.
 static inline int ilu_grid(int64_t tasks)
 {
   const int64_t ctas = (tasks + ILU_WARPS - 1) / ILU_WARPS;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(ctas, g_ilu_ctas));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(ctas, 148 * 2));
 }
 
 static double ilu_factor_bytes(cfdgpu_handle *h)
@@ -1022,9 +1023,10 @@ static int spmv64_plain(cfdgpu_handle *h, int mode, const double *x, const doubl
 // basis, Hessenberg, Givens rotations and residual on the FP64 matrix) whose
 // preconditioner is the FP32 inner solve above, x0 = 0.  The residual
 // estimate is the true residual ||b - A x||; the solve stops at
-// max(refine_rtol ||b||, T/10), T the step's Newton stopping residual, so the
-// Newton loop's FP64 residual test (element kernels in FP64) decides whether
-// the step has converged.
+// max(refine_rtol ||b||, F), F = refine_atol when set (none when negative),
+// else T/10 with T the step's Newton stopping residual.  The Newton loop's
+// FP64 residual test (element kernels in FP64) decides whether the step has
+// converged.
 static int fgmres_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_out, int *reason_out)
 {
   const int64_t n = h->n;
@@ -1040,8 +1042,10 @@ static int fgmres_mixed(cfdgpu_handle *h, const double *b, double *x, int *its_o
     return spmv64_plain(h, 0, h->Zb + (int64_t)j * h->ldv, nullptr, h->V + (int64_t)(j + 1) * h->ldv, h->gst, j);
   };
   auto res = [&]() { return spmv64_plain(h, 1, x, b, h->V, nullptr, 0); };
-  return gmres_run<double>(h, K, x, h->opts.max_it, h->refine_rtol, 0.1 * h->newton_target, h->opts.dtol, false,
-                           arn, res, its_out, reason_out);
+  const double floor = (h->opts.refine_atol > 0.0) ? h->opts.refine_atol
+                       : (h->opts.refine_atol < 0.0) ? 0.0 : 0.1 * h->newton_target;
+  return gmres_run<double>(h, K, x, h->opts.max_it, h->refine_rtol, floor, h->opts.dtol, false, arn, res, its_out,
+                           reason_out);
 }
 
 static int upload_td(cfdgpu_handle *h)
@@ -1155,7 +1159,6 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
   h->n = (int64_t)h->nNode * h->ndof;
   h->ctrl = *ctrl;
   h->opts = *opts;
-  if (const char *e = getenv("CFDGPU_ILU_CTAS")) g_ilu_ctas = std::max(1, atoi(e));
   if (h->opts.restart <= 0) h->opts.restart = 30;
   if (h->opts.restart > 1000) { h->err = "restart > 1000 is not supported"; return CFDGPU_EINVAL; }
   if (h->opts.max_it <= 0) h->opts.max_it = 10000;

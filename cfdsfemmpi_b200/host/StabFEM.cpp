@@ -152,7 +152,8 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
   opts_ = cfdgpu_solver_opts{};
   opts_.restart = 30; opts_.rtol = 1e-5; opts_.atol = 1e-50; opts_.dtol = 1e4; opts_.max_it = 10000;
   opts_.precision = CFDGPU_PREC_FP64; opts_.inner_restart = 0;
-  opts_.inner_rtol = 1e-4; opts_.reuse_tangent = 1; opts_.refine_rtol = 1e-10; opts_.newton_rtol = 0.0;
+  opts_.inner_rtol = 1e-2; opts_.inner_restart = 20; opts_.reuse_tangent = 1; opts_.refine_rtol = 1e-10;
+  opts_.newton_rtol = 0.0;
   if (ksp == "gmres") opts_.ksp_type = CFDGPU_KSP_GMRES;
   else if (ksp == "bcgs") opts_.ksp_type = CFDGPU_KSP_BCGS;
   else if (ksp == "preonly") opts_.ksp_type = CFDGPU_KSP_PREONLY;
@@ -193,6 +194,7 @@ int StabFEM::setSolver(int slv, int *parm, bool cIO)
   if (options.count("-gpu_inner_restart")) opts_.inner_restart = std::atoi(options["-gpu_inner_restart"].c_str());
   if (options.count("-gpu_inner_rtol")) opts_.inner_rtol = std::atof(options["-gpu_inner_rtol"].c_str());
   if (options.count("-gpu_refine_rtol")) opts_.refine_rtol = std::atof(options["-gpu_refine_rtol"].c_str());
+  if (options.count("-gpu_refine_atol")) opts_.refine_atol = std::atof(options["-gpu_refine_atol"].c_str());
   if (options.count("-gpu_newton_rtol")) opts_.newton_rtol = std::atof(options["-gpu_newton_rtol"].c_str());
   {
     const std::string f = get("-gpu_formulation", "semi_implicit");

@@ -23,7 +23,8 @@ implement raises ``io.InputError`` instead of being replaced by another method.
 Library keys:
 
   -gpu_precision fp64|mixed   -gpu_inner_restart m    -gpu_inner_rtol r
-  -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_newton_rtol r
+  -gpu_reuse_tangent 0|1      -gpu_refine_rtol r      -gpu_refine_atol a
+  -gpu_newton_rtol r
   -gpu_formulation semi_implicit|fully_implicit   (element routine; the
         reference's active one, or its commented-out fully-implicit one)
   -gpu_guess constant|extrapolation   (Newton initial guess; constant = the
@@ -87,6 +88,8 @@ def solver_options_from_petsc(opts: Dict[str, str]) -> Dict:
         kw["reuse_tangent"] = bool(int(opts["-gpu_reuse_tangent"]))
     if "-gpu_refine_rtol" in opts:
         kw["refine_rtol"] = float(opts["-gpu_refine_rtol"])
+    if "-gpu_refine_atol" in opts:
+        kw["refine_atol"] = float(opts["-gpu_refine_atol"])
     if "-gpu_newton_rtol" in opts:
         kw["newton_rtol"] = float(opts["-gpu_newton_rtol"])
     if "-gpu_guess" in opts:

@@ -107,8 +107,8 @@ typedef struct cfdgpu_solver_opts {
   int inner_restart;        /* mixed mode: FP32 BiCGStab iterations per outer flexible-GMRES step (0: 20) */
   double inner_rtol;        /* mixed mode: inner relative tolerance of those iterations (0: 1e-2) */
   int reuse_tangent;        /* 1: assemble K once per step, residual-only after (exact for this formulation) */
-  double refine_rtol;       /* mixed mode: outer target ||b - A x|| <= max(refine_rtol ||b||, T/10) on the FP64
-                               matrix, T the step's Newton target below (0: 1e-10); restart = outer restart */
+  double refine_rtol;       /* mixed mode: outer target ||b - A x|| <= max(refine_rtol ||b||, F) on the FP64
+                               matrix, F below (0: 1e-10); restart = outer restart */
   double newton_rtol;       /* extra relative Newton test ||F_k|| <= newton_rtol ||F_0||, F_0 the iteration-0
                                residual of the constant predictor (0: off, the reference's test only) */
   int formulation;          /* CFDGPU_FORM_*: element routine (0: the reference's active semi-implicit one) */
@@ -116,6 +116,8 @@ typedef struct cfdgpu_solver_opts {
   int ilu_levels;           /* CFDGPU_PC_BJACOBI_ILU: level of fill k (-sub_pc_factor_levels, 0..16); -1 keeps
                                all fill: the complete block LU of each block (-pc_type lu, natural ordering) */
   int bjacobi_blocks;       /* CFDGPU_PC_BJACOBI_ILU: number of blocks (0 or 1: one block, as a serial run) */
+  double refine_atol;       /* mixed mode: absolute floor F of the outer target max(refine_rtol ||b||, F)
+                               (0: T/10, T the step's Newton target; < 0: no floor) */
 } cfdgpu_solver_opts;
 
 /* element formulations */
