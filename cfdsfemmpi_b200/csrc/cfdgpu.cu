@@ -445,13 +445,16 @@ static int assemble(cfdgpu_handle *h, int iter, bool want_K)
   return 0;
 }
 
-// Persistent grid of the sync-free ILU kernels: enough warps for `tasks`
-// rows, at most 2 CTAs of 8 warps per SM.  More warps in flight only add
-// polling traffic: on the 115^3 cavity the triangular-solve pair takes 5.4 ms
-// with 2 CTAs per SM against 9.5 ms with 4 and 14 ms with 8.
-static inline int ilu_grid(int64_t tasks)
+// Persistent grid of the sync-free ILU kernels: warps in flight for `tasks`
+// rows whose widest dependency level holds `width` rows.  Warps beyond what
+// the levels can feed only add polling traffic: on the 115^3 cavity the
+// triangular-solve pair takes 5.4 ms with 2 CTAs of 8 warps per SM against
+// 9.5 ms with 4 and 14 ms with 8, and a chain of single-row levels (the
+// complete factorisation of a band) needs a few dozen warps, not thousands.
+static inline int ilu_grid(int64_t tasks, int64_t width)
 {
-  const int64_t ctas = (tasks + ILU_WARPS - 1) / ILU_WARPS;
+  const int64_t warps = std::min<int64_t>(tasks, std::max<int64_t>(256, 2 * width));
+  const int64_t ctas = (warps + ILU_WARPS - 1) / ILU_WARPS;
   return (int)std::max<int64_t>(1, std::min<int64_t>(ctas, 148 * 2));
 }
 
@@ -475,7 +478,7 @@ static double trsv_bytes(cfdgpu_handle *h)
 static int ilu_factor_run32(cfdgpu_handle *h)
 {
   const int pi = prof_begin(h, CFDGPU_KIND_ILU, 0.5 * ilu_factor_bytes(h));
-  const int grid = ilu_grid(h->nNode);
+  const int grid = ilu_grid(h->nNode, h->ilu.maxw_l);
   if (h->ndof == 4)
     ilu_factor<4, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr32, h->frow,
                                                                     h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
@@ -494,7 +497,7 @@ static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresSt
 {
   if ((const void *)r == (const void *)z) { h->err = "ILU apply: input and output overlap"; return CFDGPU_EINVAL; }
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, 0.5 * trsv_bytes(h));
-  const int grid = ilu_grid(h->nNode);
+  const int grid = ilu_grid(h->nNode, std::max(h->ilu.maxw_l, h->ilu.maxw_u));
 #define TRSV32(NB)                                                                                              \
   ilu_trsv<NB, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->florder, h->frow, h->fcol, \
       h->fdiag, h->fval32, h->fdinv32, r, h->ybuf32, z, h->tctl, st, j, active);                               \
@@ -511,7 +514,7 @@ static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresSt
 static int ilu_factor_run(cfdgpu_handle *h)
 {
   const int pi = prof_begin(h, CFDGPU_KIND_ILU, ilu_factor_bytes(h));
-  const int grid = ilu_grid(h->nNode);
+  const int grid = ilu_grid(h->nNode, h->ilu.maxw_l);
   if (h->ndof == 4)
     ilu_factor<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
                                                                       h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
@@ -530,7 +533,7 @@ static int ilu_apply(cfdgpu_handle *h, const double *r, double *z, const GmresSt
 {
   if ((const void *)r == (const void *)z) { h->err = "ILU apply: input and output overlap"; return CFDGPU_EINVAL; }
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, trsv_bytes(h));
-  const int grid = ilu_grid(h->nNode);
+  const int grid = ilu_grid(h->nNode, std::max(h->ilu.maxw_l, h->ilu.maxw_u));
 #define TRSV64(NB)                                                                                                \
   ilu_trsv<NB, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->florder, h->frow, h->fcol, \
       h->fdiag, h->fval, h->fdinv, r, h->ybuf, z, h->tctl, st, j, active);                                         \

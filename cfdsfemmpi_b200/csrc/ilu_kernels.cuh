@@ -386,32 +386,9 @@ ilu_trsv(int n, const int32_t *__restrict__ order, const int32_t *__restrict__ f
       }
 #pragma unroll
       for (int k = 0; k < TRSV_BATCH; k++) v[k] = (p[k] >= 0) ? S::load(src + (int64_t)p[k] * NB + ec) : 0;
-      // inputs not written yet: one lane of the warp polls (the lowest lane
-      // with a missing input, on its first one), the others wait at the warp
-      // barrier and reload afterwards, so a waiting warp costs one poller
-      while (true) {
-        int miss = -1;
-#pragma unroll
-        for (int k = TRSV_BATCH - 1; k >= 0; k--)
-          if (p[k] >= 0 && v[k] == S::bits) miss = k;
-        const unsigned int m = __ballot_sync(0xffffffffu, miss >= 0);
-        if (!m) break;
-        if (lane == __ffs(m) - 1) {
-          const VT *addr = src + (int64_t)p[0] * NB + ec;
-#pragma unroll
-          for (int k = 0; k < TRSV_BATCH; k++)
-            if (k == miss) addr = src + (int64_t)p[k] * NB + ec;
-          (void)wait_value<VT>(addr, S::bits, ctl);
-        }
-        __syncwarp();
-        if (*(volatile unsigned int *)&ctl->error) break;
-#pragma unroll
-        for (int k = 0; k < TRSV_BATCH; k++)
-          if (p[k] >= 0 && v[k] == S::bits) v[k] = S::load(src + (int64_t)p[k] * NB + ec);
-      }
 #pragma unroll
       for (int k = 0; k < TRSV_BATCH; k++)
-        if (p[k] >= 0) acc = fma(a[k], (double)S::value(v[k]), acc);
+        if (p[k] >= 0) acc = fma(a[k], wait_value<VT>(src + (int64_t)p[k] * NB + ec, v[k], ctl), acc);
     }
     red[w][lane] = acc;
     __syncwarp();

@@ -217,11 +217,13 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
   // level-set orders of the lower and upper dependency DAGs
   {
     std::vector<int32_t> lev(n, 0);
-    auto order_by = [&](std::vector<int32_t> &out) {
+    auto order_by = [&](std::vector<int32_t> &out, int &maxw) {
       int nl = 0;
       for (int i = 0; i < n; i++) nl = std::max(nl, lev[i] + 1);
       std::vector<int32_t> cnt(nl + 1, 0);
       for (int i = 0; i < n; i++) cnt[lev[i] + 1]++;
+      maxw = 0;
+      for (int k = 0; k < nl; k++) maxw = std::max(maxw, cnt[k + 1]);
       for (int k = 0; k < nl; k++) cnt[k + 1] += cnt[k];
       out.resize(n);
       for (int i = 0; i < n; i++) out[cnt[lev[i]]++] = i;
@@ -232,13 +234,13 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
       for (int q = f.rowptr[i]; q < f.diag[i]; q++) d = std::max(d, lev[f.colidx[q]] + 1);
       lev[i] = d;
     }
-    f.nlev_l = order_by(f.lorder);
+    f.nlev_l = order_by(f.lorder, f.maxw_l);
     for (int i = n - 1; i >= 0; i--) {
       int d = 0;
       for (int q = f.diag[i] + 1; q < f.rowptr[i + 1]; q++) d = std::max(d, lev[f.colidx[q]] + 1);
       lev[i] = d;
     }
-    f.nlev_u = order_by(f.uorder);
+    f.nlev_u = order_by(f.uorder, f.maxw_u);
   }
   // update map: positions in row i of the upper blocks of every pivot row
   {

@@ -70,6 +70,7 @@ struct IluPattern {
   // the upper DAG (upper solve), row order inside a level
   std::vector<int32_t> lorder, uorder;
   int nlev_l = 0, nlev_u = 0;
+  int maxw_l = 0, maxw_u = 0;    // rows in the widest level of each DAG
   int64_t nnzb() const { return (int64_t)colidx.size(); }
 };
 
