@@ -118,6 +118,7 @@ struct cfdgpu_handle {
   IluPattern ilu;
   int32_t *frow = nullptr, *fcol = nullptr, *fdiag = nullptr, *faslot = nullptr, *fumap = nullptr;
   int32_t *florder = nullptr, *fuorder = nullptr;
+  int32_t *flchain = nullptr, *fuchain = nullptr, *flchord = nullptr, *fuchord = nullptr, *fperm = nullptr;
   int64_t *fuoff = nullptr;
   double *fval = nullptr, *fdinv = nullptr;
   unsigned int *iflags = nullptr;
@@ -481,11 +482,11 @@ static int ilu_factor_run32(cfdgpu_handle *h)
   const int grid = ilu_grid(h->nNode, h->ilu.maxw_l);
   if (h->ndof == 4)
     ilu_factor<4, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr32, h->frow,
-                                                                    h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                    h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder, h->fperm,
                                                                     h->fval32, h->fdinv32, h->iflags, h->tctl);
   else
     ilu_factor<3, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr32, h->frow,
-                                                                    h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                    h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder, h->fperm,
                                                                     h->fval32, h->fdinv32, h->iflags, h->tctl);
   prof_end(h, pi);
   LAUNCHED(h);
@@ -497,12 +498,14 @@ static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresSt
 {
   if ((const void *)r == (const void *)z) { h->err = "ILU apply: input and output overlap"; return CFDGPU_EINVAL; }
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, 0.5 * trsv_bytes(h));
-  const int grid = ilu_grid(h->nNode, std::max(h->ilu.maxw_l, h->ilu.maxw_u));
+  const int nl = (int)h->ilu.lchain_order.size(), nu = (int)h->ilu.uchain_order.size();
+  // every chain of a wavefront band is in flight at once: up to one warp per chain
+  const int gl = ilu_grid(nl, nl), gu = ilu_grid(nu, nu);
 #define TRSV32(NB)                                                                                              \
-  ilu_trsv<NB, false, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->florder, h->frow, h->fcol, \
-      h->fdiag, h->fval32, h->fdinv32, r, h->ybuf32, z, h->tctl, st, j, active);                               \
-  ilu_trsv<NB, true, float, float><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->fuorder, h->frow, h->fcol,  \
-      h->fdiag, h->fval32, h->fdinv32, nullptr, h->ybuf32, z, h->tctl, st, j, active)
+  ilu_trsv<NB, false, float, float><<<gl, ILU_THREADS, 0, h->stream>>>(nl, h->flchord, h->flchain, h->frow,       \
+      h->fcol, h->fdiag, h->fval32, h->fdinv32, h->fperm, r, h->ybuf32, z, h->tctl, st, j, active);                      \
+  ilu_trsv<NB, true, float, float><<<gu, ILU_THREADS, 0, h->stream>>>(nu, h->fuchord, h->fuchain, h->frow,        \
+      h->fcol, h->fdiag, h->fval32, h->fdinv32, h->fperm, nullptr, h->ybuf32, z, h->tctl, st, j, active);
   if (h->ndof == 4) { TRSV32(4); } else { TRSV32(3); }
 #undef TRSV32
   prof_end(h, pi);
@@ -517,11 +520,11 @@ static int ilu_factor_run(cfdgpu_handle *h)
   const int grid = ilu_grid(h->nNode, h->ilu.maxw_l);
   if (h->ndof == 4)
     ilu_factor<4, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
-                                                                      h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                      h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder, h->fperm,
                                                                       h->fval, h->fdinv, h->iflags, h->tctl);
   else
     ilu_factor<3, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->rowptr, h->faslot, h->bsr, h->frow,
-                                                                      h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder,
+                                                                      h->fcol, h->fdiag, h->fuoff, h->fumap, h->florder, h->fperm,
                                                                       h->fval, h->fdinv, h->iflags, h->tctl);
   prof_end(h, pi);
   LAUNCHED(h);
@@ -533,12 +536,14 @@ static int ilu_apply(cfdgpu_handle *h, const double *r, double *z, const GmresSt
 {
   if ((const void *)r == (const void *)z) { h->err = "ILU apply: input and output overlap"; return CFDGPU_EINVAL; }
   const int pi = prof_begin(h, CFDGPU_KIND_TRSV, trsv_bytes(h));
-  const int grid = ilu_grid(h->nNode, std::max(h->ilu.maxw_l, h->ilu.maxw_u));
+  const int nl = (int)h->ilu.lchain_order.size(), nu = (int)h->ilu.uchain_order.size();
+  // every chain of a wavefront band is in flight at once: up to one warp per chain
+  const int gl = ilu_grid(nl, nl), gu = ilu_grid(nu, nu);
 #define TRSV64(NB)                                                                                                \
-  ilu_trsv<NB, false, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->florder, h->frow, h->fcol, \
-      h->fdiag, h->fval, h->fdinv, r, h->ybuf, z, h->tctl, st, j, active);                                         \
-  ilu_trsv<NB, true, double, double><<<grid, ILU_THREADS, 0, h->stream>>>(h->nNode, h->fuorder, h->frow, h->fcol,  \
-      h->fdiag, h->fval, h->fdinv, nullptr, h->ybuf, z, h->tctl, st, j, active)
+  ilu_trsv<NB, false, double, double><<<gl, ILU_THREADS, 0, h->stream>>>(nl, h->flchord, h->flchain, h->frow,       \
+      h->fcol, h->fdiag, h->fval, h->fdinv, h->fperm, r, h->ybuf, z, h->tctl, st, j, active);                              \
+  ilu_trsv<NB, true, double, double><<<gu, ILU_THREADS, 0, h->stream>>>(nu, h->fuchord, h->fuchain, h->frow,        \
+      h->fcol, h->fdiag, h->fval, h->fdinv, h->fperm, nullptr, h->ybuf, z, h->tctl, st, j, active);
   if (h->ndof == 4) { TRSV64(4); } else { TRSV64(3); }
 #undef TRSV64
   prof_end(h, pi);
@@ -1296,6 +1301,11 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
     if ((rc = upload(h, &h->fumap, f.umap.data(), f.umap.size()))) return rc;
     if ((rc = upload(h, &h->florder, f.lorder.data(), f.lorder.size()))) return rc;
     if ((rc = upload(h, &h->fuorder, f.uorder.data(), f.uorder.size()))) return rc;
+    if ((rc = upload(h, &h->flchain, f.lchain.data(), f.lchain.size()))) return rc;
+    if ((rc = upload(h, &h->fuchain, f.uchain.data(), f.uchain.size()))) return rc;
+    if ((rc = upload(h, &h->flchord, f.lchain_order.data(), f.lchain_order.size()))) return rc;
+    if ((rc = upload(h, &h->fuchord, f.uchain_order.data(), f.uchain_order.size()))) return rc;
+    if (!f.perm.empty() && (rc = upload(h, &h->fperm, f.perm.data(), f.perm.size()))) return rc;
     if (h->mixed) {
       if ((rc = dalloc(h, &h->fval32, (size_t)f.nnzb() * bb))) return rc;
       CK(cudaMemset(h->fval32, 0, sizeof(float) * f.nnzb() * bb));

@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(ILU_THREADS)
 ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ aslot, const AT *__restrict__ aval,
            const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol, const int32_t *__restrict__ fdiag,
            const int64_t *__restrict__ uoff, const int32_t *__restrict__ umap, const int32_t *__restrict__ order,
-           FT *fval, FT *fdinv, unsigned int *flags, TriCtl *ctl)
+           const int32_t *__restrict__ perm, FT *fval, FT *fdinv, unsigned int *flags, TriCtl *ctl)
 {
   constexpr int BB = NB * NB;
   constexpr int G = 32 / BB;          // blocks per warp step
@@ -184,7 +184,8 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
     for (int64_t x = (int64_t)f0 * BB + lane; x < (int64_t)f1 * BB; x += 32) fval[x] = FT(0);
     __syncwarp();
     {
-      const int a0 = arow[i], a1 = arow[i + 1];
+      const int ai = perm ? perm[i] : i;   // node of factor row i
+      const int a0 = arow[ai], a1 = arow[ai + 1];
       for (int64_t x = lane; x < (int64_t)(a1 - a0) * BB; x += 32) {
         const int k = a0 + (int)(x / BB);
         const int s = aslot[k];
@@ -260,8 +261,7 @@ ilu_factor(int n, const int32_t *__restrict__ arow, const int32_t *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Triangular solves z = (L U)^-1 r, one warp per row, rows in level order
-// (lorder for the lower solve, uorder for the upper solve).
+// Triangular solves z = (L U)^-1 r.
 //
 // The values are their own ready flags: the intermediate vector y and the
 // output z hold a signalling-NaN sentinel (a bit pattern no arithmetic
@@ -342,11 +342,22 @@ __global__ void fill_sentinel_f32(int64_t n, float *y)
 }
 
 constexpr int TRSV_BATCH = 4;   // input loads in flight per lane
+constexpr int TRSV_CHAIN_MAX = 128;
 
+// One warp per chain of rows (see IluPattern::lchain / uchain), chains in
+// level order of the chain DAG.  The chain's rows are solved in order; inputs
+// from the chain itself come from shared memory, inputs from other chains
+// from global memory once they are no longer the sentinel.
+//
+// Lower:  y_i = r_P(i) - sum_{p<i} L_ip y_p
+// Upper:  z_P(i) = U_ii^-1 (y_i - sum_{p>i} U_ip z_P(p))
+// with P the factor's row order (perm; NULL: the identity): y is indexed by
+// factor row, r and z by node.
 template <int NB, bool UPPER, typename FT, typename VT>
 __global__ void __launch_bounds__(ILU_THREADS)
-ilu_trsv(int n, const int32_t *__restrict__ order, const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol,
-         const int32_t *__restrict__ fdiag, const FT *__restrict__ fval, const FT *__restrict__ fdinv, const VT *r,
+ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restrict__ chains,
+         const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol, const int32_t *__restrict__ fdiag,
+         const FT *__restrict__ fval, const FT *__restrict__ fdinv, const int32_t *__restrict__ perm, const VT *r,
          VT *y, VT *z, TriCtl *ctl, const GmresState *__restrict__ st, int j, const int *__restrict__ active)
 {
   if (st && (!st->active || st->it != j)) return;
@@ -357,63 +368,83 @@ ilu_trsv(int n, const int32_t *__restrict__ order, const int32_t *__restrict__ f
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   __shared__ double red[ILU_WARPS][32];
   __shared__ double sv[ILU_WARPS][NB];
+  __shared__ double cache[ILU_WARPS][TRSV_CHAIN_MAX * NB];
   const unsigned int epoch = *(volatile unsigned int *)&ctl->epoch;
   const int g = lane / BB, e = lane % BB, ec = e % NB;
   // the vector the off-diagonal products read: y (lower) or z (upper)
   const VT *src = UPPER ? z : y;
   while (true) {
     const int tk = draw_ticket(ctl, lane);
-    if (tk >= n) break;
-    const int i = order[tk];
-    const int q0 = UPPER ? fdiag[i] + 1 : fptr[i];
-    const int q1 = UPPER ? fptr[i + 1] : fdiag[i];
-    // visit the row's blocks so that the nearest column (i-1 below the
-    // diagonal, i+1 above it: the input finished last) comes last, and the
-    // other products accumulate while it is still being computed
-    double acc = 0.0;
-    const int nq = q1 - q0;
-    for (int qb = 0; qb < nq; qb += G * TRSV_BATCH) {
-      typename S::U v[TRSV_BATCH];
-      int p[TRSV_BATCH];
-      double a[TRSV_BATCH];
+    if (tk >= nchains) break;
+    const int c = order[tk];
+    const int lo = chains[2 * c], hi = chains[2 * c + 1];
+    for (int step = 0; step < hi - lo; step++) {
+      const int i = UPPER ? hi - 1 - step : lo + step;
+      const int q0 = UPPER ? fdiag[i] + 1 : fptr[i];
+      const int q1 = UPPER ? fptr[i + 1] : fdiag[i];
+      // blocks in the order farthest column first, so the chain's own
+      // previous row (the input finished last) is consumed last
+      double acc = 0.0;
+      const int nq = q1 - q0;
+      for (int qb = 0; qb < nq; qb += G * TRSV_BATCH) {
+        typename S::U v[TRSV_BATCH];
+        int p[TRSV_BATCH];
+        double a[TRSV_BATCH];
+        bool own[TRSV_BATCH];
 #pragma unroll
-      for (int k = 0; k < TRSV_BATCH; k++) {
-        const int qq = qb + k * G + g;
-        const bool ok = (g < G && qq < nq);
-        const int q = UPPER ? q1 - 1 - qq : q0 + qq;
-        p[k] = ok ? fcol[q] : -1;
-        a[k] = ok ? (double)fval[(int64_t)q * BB + e] : 0.0;
+        for (int k = 0; k < TRSV_BATCH; k++) {
+          const int qq = qb + k * G + g;
+          const bool ok = (g < G && qq < nq);
+          const int q = UPPER ? q1 - 1 - qq : q0 + qq;
+          p[k] = ok ? fcol[q] : -1;
+          a[k] = ok ? (double)fval[(int64_t)q * BB + e] : 0.0;
+          own[k] = ok && (UPPER ? p[k] < hi : p[k] >= lo);
+        }
+        // z is indexed by node, y by factor row
+        int64_t at[TRSV_BATCH];
+#pragma unroll
+        for (int k = 0; k < TRSV_BATCH; k++)
+          at[k] = (int64_t)((UPPER && perm && p[k] >= 0) ? perm[p[k]] : p[k]) * NB + ec;
+#pragma unroll
+        for (int k = 0; k < TRSV_BATCH; k++) v[k] = (p[k] >= 0 && !own[k]) ? S::load(src + at[k]) : 0;
+#pragma unroll
+        for (int k = 0; k < TRSV_BATCH; k++) {
+          if (p[k] < 0) continue;
+          const double xv = own[k] ? cache[w][(UPPER ? hi - 1 - p[k] : p[k] - lo) * NB + ec]
+                                   : wait_value<VT>(src + at[k], v[k], ctl);
+          acc = fma(a[k], xv, acc);
+        }
       }
+      red[w][lane] = acc;
+      __syncwarp();
+      const int64_t node = perm ? perm[i] : i;
+      if (lane < NB) {
+        double s = UPPER ? (double)y[(int64_t)i * NB + lane] : (double)r[node * NB + lane];
 #pragma unroll
-      for (int k = 0; k < TRSV_BATCH; k++) v[k] = (p[k] >= 0) ? S::load(src + (int64_t)p[k] * NB + ec) : 0;
+        for (int gg = 0; gg < G; gg++)
 #pragma unroll
-      for (int k = 0; k < TRSV_BATCH; k++)
-        if (p[k] >= 0) acc = fma(a[k], wait_value<VT>(src + (int64_t)p[k] * NB + ec, v[k], ctl), acc);
-    }
-    red[w][lane] = acc;
-    __syncwarp();
-    if (lane < NB) {
-      double s = UPPER ? (double)y[(int64_t)i * NB + lane] : (double)r[(int64_t)i * NB + lane];
-#pragma unroll
-      for (int gg = 0; gg < G; gg++)
-#pragma unroll
-        for (int c = 0; c < NB; c++) s -= red[w][gg * BB + lane * NB + c];
-      sv[w][lane] = s;
-    }
-    __syncwarp();
-    if (lane < NB) {
-      if (UPPER) {
-        double v = 0.0;
-#pragma unroll
-        for (int c = 0; c < NB; c++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + c], sv[w][c], v);
-        S::store(z + (int64_t)i * NB + lane, (VT)v);
-        y[(int64_t)i * NB + lane] = S::sentinel();
-      } else {
-        z[(int64_t)i * NB + lane] = S::sentinel();
-        S::store(y + (int64_t)i * NB + lane, (VT)sv[w][lane]);
+          for (int cc = 0; cc < NB; cc++) s -= red[w][gg * BB + lane * NB + cc];
+        sv[w][lane] = s;
       }
+      __syncwarp();
+      if (lane < NB) {
+        if (UPPER) {
+          double v = 0.0;
+#pragma unroll
+          for (int cc = 0; cc < NB; cc++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + cc], sv[w][cc], v);
+          const VT vv = (VT)v;
+          cache[w][step * NB + lane] = (double)vv;
+          S::store(z + node * NB + lane, vv);
+          y[(int64_t)i * NB + lane] = S::sentinel();
+        } else {
+          const VT vv = (VT)sv[w][lane];
+          cache[w][step * NB + lane] = (double)vv;
+          z[node * NB + lane] = S::sentinel();
+          S::store(y + (int64_t)i * NB + lane, vv);
+        }
+      }
+      __syncwarp();
     }
-    __syncwarp();
   }
   launch_done(ctl, lane, epoch);
 }

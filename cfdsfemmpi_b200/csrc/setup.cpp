@@ -158,10 +158,42 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
     for (int b = 0; b <= nb; b++) f.blk[b] = b * q + std::min(b, r);
   }
   const uint8_t all = (uint8_t)((1u << t.ndof) - 1u);
-  auto fixed_node = [&](int v) { return (t.fixmask[v] & all) == all; };
+  auto fixed_node0 = [&](int v) { return (t.fixmask[v] & all) == all; };
+  if (f.levels < 0 && nb == 1) {
+    // reverse Cuthill-McKee: breadth-first from a minimum-degree node of each
+    // component, neighbours in increasing degree, the whole order reversed
+    std::vector<int32_t> deg(n), order;
+    order.reserve(n);
+    for (int v = 0; v < n; v++) deg[v] = t.rowptr[v + 1] - t.rowptr[v];
+    std::vector<uint8_t> seen(n, 0);
+    std::vector<int32_t> nbr;
+    while ((int)order.size() < n) {
+      int s0 = -1;
+      for (int v = 0; v < n; v++)
+        if (!seen[v] && (s0 < 0 || deg[v] < deg[s0])) s0 = v;
+      seen[s0] = 1;
+      size_t head = order.size();
+      order.push_back(s0);
+      while (head < order.size()) {
+        const int v = order[head++];
+        nbr.clear();
+        for (int k = t.rowptr[v]; k < t.rowptr[v + 1]; k++)
+          if (!seen[t.colidx[k]]) { seen[t.colidx[k]] = 1; nbr.push_back(t.colidx[k]); }
+        std::stable_sort(nbr.begin(), nbr.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+        order.insert(order.end(), nbr.begin(), nbr.end());
+      }
+    }
+    f.perm.assign(order.rbegin(), order.rend());
+    f.iperm.resize(n);
+    for (int i = 0; i < n; i++) f.iperm[f.perm[i]] = i;
+  }
+  auto P = [&](int i) { return f.perm.empty() ? i : f.perm[i]; };    // factor row -> node
+  auto IP = [&](int v) { return f.iperm.empty() ? v : f.iperm[v]; };  // node -> factor row
+  auto fixed_node = [&](int i) { return fixed_node0(P(i)); };
   std::vector<int32_t> blk_of(n);
   for (int b = 0; b < nb; b++)
     for (int v = f.blk[b]; v < f.blk[b + 1]; v++) blk_of[v] = b;
+  std::vector<int32_t> rowcols;
   // per-row sorted linked list over column nodes (n = end marker)
   std::vector<int32_t> next(n + 1), lv(n);
   std::vector<int32_t> ulev;       // level of every stored entry
@@ -179,11 +211,15 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
     if (fixed_node(i)) {
       push(i);
     } else {
-      for (int k = t.rowptr[i]; k < t.rowptr[i + 1]; k++) {
-        const int c = t.colidx[k];
+      const int v = P(i);
+      rowcols.clear();
+      for (int k = t.rowptr[v]; k < t.rowptr[v + 1]; k++) {
+        const int c = IP(t.colidx[k]);
         if (blk_of[c] != blk_of[i] || (c != i && fixed_node(c))) continue;
-        push(c);
+        rowcols.push_back(c);
       }
+      std::sort(rowcols.begin(), rowcols.end());
+      for (int c : rowcols) push(c);
     }
     if (tail >= 0) next[tail] = n;
     for (int p = head; p < i; p = next[p]) {
@@ -242,6 +278,58 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
     }
     f.nlev_u = order_by(f.uorder, f.maxw_u);
   }
+  // chains of the lower (ascending) and upper (descending) solves and their
+  // DAG levels
+  {
+    auto chains = [&](bool upper, std::vector<int32_t> &ch, std::vector<int32_t> &order, int &nlev, int &maxw) {
+      ch.clear();
+      std::vector<int32_t> chain_of(n);
+      if (!upper) {
+        int start = 0;
+        for (int i = 1; i <= n; i++) {
+          const bool cont = i < n && i - start < ILU_CHAIN_MAX && f.diag[i] > f.rowptr[i] &&
+                            f.colidx[f.diag[i] - 1] == i - 1;
+          if (!cont) { ch.push_back(start); ch.push_back(i); start = i; }
+        }
+      } else {
+        int end = n;   // current chain covers [i, end)
+        for (int i = n - 2; i >= -1; i--) {
+          const int r = i + 1;   // row just added
+          const bool cont = i >= 0 && end - i <= ILU_CHAIN_MAX && f.diag[i] + 1 < f.rowptr[i + 1] &&
+                            f.colidx[f.diag[i] + 1] == i + 1;
+          if (!cont) { ch.push_back(r); ch.push_back(end); end = r; }
+        }
+      }
+      const int nc = (int)ch.size() / 2;
+      for (int c = 0; c < nc; c++)
+        for (int i = ch[2 * c]; i < ch[2 * c + 1]; i++) chain_of[i] = c;
+      std::vector<int32_t> lev(nc, 0);
+      // chains are listed in dependency order (ascending rows for the lower
+      // solve, descending for the upper one), so one pass finds the levels
+      for (int c = 0; c < nc; c++) {
+        int d = 0;
+        for (int i = ch[2 * c]; i < ch[2 * c + 1]; i++) {
+          const int q0 = upper ? f.diag[i] + 1 : f.rowptr[i], q1 = upper ? f.rowptr[i + 1] : f.diag[i];
+          for (int q = q0; q < q1; q++) {
+            const int oc = chain_of[f.colidx[q]];
+            if (oc != c) d = std::max(d, lev[oc] + 1);
+          }
+        }
+        lev[c] = d;
+      }
+      nlev = 0;
+      for (int c = 0; c < nc; c++) nlev = std::max(nlev, lev[c] + 1);
+      std::vector<int32_t> cnt(nlev + 1, 0);
+      for (int c = 0; c < nc; c++) cnt[lev[c] + 1]++;
+      maxw = 0;
+      for (int k = 0; k < nlev; k++) maxw = std::max(maxw, cnt[k + 1]);
+      for (int k = 0; k < nlev; k++) cnt[k + 1] += cnt[k];
+      order.resize(nc);
+      for (int c = 0; c < nc; c++) order[cnt[lev[c]]++] = c;
+    };
+    chains(false, f.lchain, f.lchain_order, f.lchain_levels, f.lchain_maxw);
+    chains(true, f.uchain, f.uchain_order, f.uchain_levels, f.uchain_maxw);
+  }
   // update map: positions in row i of the upper blocks of every pivot row
   {
     int64_t total = 0;
@@ -264,13 +352,16 @@ std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPat
       for (int k = f.rowptr[i]; k < f.rowptr[i + 1]; k++) pos[f.colidx[k]] = -1;
     }
   }
-  // blocks of A inside the factor pattern
+  // blocks of A inside the factor pattern (A's block (v, c) lands in factor
+  // row IP(v) at column IP(c))
   f.aslot.assign(t.colidx.size(), -1);
-  for (int i = 0; i < n; i++) {
+  for (int v = 0; v < n; v++) {
+    const int i = IP(v);
     const int32_t *b = f.colidx.data() + f.rowptr[i], *e = f.colidx.data() + f.rowptr[i + 1];
-    for (int k = t.rowptr[i]; k < t.rowptr[i + 1]; k++) {
-      const int32_t *p = std::lower_bound(b, e, t.colidx[k]);
-      if (p != e && *p == t.colidx[k]) f.aslot[k] = (int32_t)(p - f.colidx.data());
+    for (int k = t.rowptr[v]; k < t.rowptr[v + 1]; k++) {
+      const int c = IP(t.colidx[k]);
+      const int32_t *p = std::lower_bound(b, e, c);
+      if (p != e && *p == c) f.aslot[k] = (int32_t)(p - f.colidx.data());
     }
   }
   return "";

@@ -60,6 +60,12 @@ struct IluPattern {
   std::vector<int32_t> diag;     // position of the diagonal block of each row
   std::vector<int32_t> aslot;    // per block of A: its position in the factors, or -1
   std::vector<int32_t> blk;      // nblocks+1 node offsets
+  // factor row i is node perm[i] (empty: the identity).  ILU(k) keeps the
+  // natural order, as PETSc's ILU does; the complete factorisation of one
+  // block (-pc_type lu) uses a reverse Cuthill-McKee order of the node graph,
+  // which bounds its fill by the graph's bandwidth (a direct solve's result
+  // does not depend on the order beyond rounding)
+  std::vector<int32_t> perm, iperm;
   // update map of the numeric factorisation: for a strictly lower block q =
   // (i, p), umap[uoff[q] + k] is the position in row i of the k-th block
   // right of the diagonal in row p, or -1 when row i's pattern drops it
@@ -71,8 +77,19 @@ struct IluPattern {
   std::vector<int32_t> lorder, uorder;
   int nlev_l = 0, nlev_u = 0;
   int maxw_l = 0, maxw_u = 0;    // rows in the widest level of each DAG
+  // chains of the triangular solves: maximal runs of consecutive rows in
+  // which each row depends on its neighbour (row i on i-1 in the lower solve,
+  // on i+1 in the upper solve), at most ILU_CHAIN_MAX rows.  A chain is solved
+  // in order by one warp, so the dependency along it never goes through
+  // memory.  lchain/uchain: nchains x {first row, one past the last row};
+  // lchain_order/uchain_order: chain ids sorted by the level of the chain
+  // DAG (a chain's inputs lie in chains of lower levels).
+  std::vector<int32_t> lchain, uchain, lchain_order, uchain_order;
+  int lchain_levels = 0, uchain_levels = 0, lchain_maxw = 0, uchain_maxw = 0;
   int64_t nnzb() const { return (int64_t)colidx.size(); }
 };
+
+constexpr int ILU_CHAIN_MAX = 128;
 
 std::string build_ilu_pattern(const Topology &t, int levels, int nblocks, IluPattern &f);
 
