@@ -322,18 +322,20 @@ __global__ void k_round_f32(int64_t n4, const double *__restrict__ a, float *__r
 // zero dof d of every node
 __global__ void k_zero_dof(int nNode, int ndof, int d, double *__restrict__ v)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nNode) v[(int64_t)i * ndof + d] = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nNode; i += (int64_t)gridDim.x * blockDim.x)
+    v[i * ndof + d] = 0.0;
 }
 
 // d = a - b on free dofs, 0 on prescribed ones
 __global__ void k_diff_free(int nNode, int ndof, const double *__restrict__ a, const double *__restrict__ b,
                             const uint8_t *__restrict__ fixmask, double *__restrict__ d)
 {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)nNode * ndof) return;
-  const int node = (int)(t / ndof), dof = (int)(t % ndof);
-  d[t] = ((fixmask[node] >> dof) & 1u) ? 0.0 : a[t] - b[t];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)nNode * ndof;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t node = t / ndof;
+    const int dof = (int)(t % ndof);
+    d[t] = ((fixmask[node] >> dof) & 1u) ? 0.0 : a[t] - b[t];
+  }
 }
 
 // y = a*x + b*y
@@ -349,6 +351,8 @@ __global__ void k_axpy(int64_t n, double a, const double *__restrict__ x, double
     y[i] += a * x[i];
 }
 
+// Blocks for an elementwise kernel over n entries, at most `cap`: every
+// kernel launched with it loops over its range with a grid stride.
 static inline int grid_for(int64_t n, int bs = 256, int cap = 148 * 16)
 {
   int64_t g = (n + bs - 1) / bs;

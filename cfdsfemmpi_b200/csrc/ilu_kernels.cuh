@@ -44,6 +44,12 @@ constexpr unsigned int ILU_ERR_ZERO_PIVOT = 2u;  // singular diagonal block in t
 constexpr int ILU_THREADS = 256;
 constexpr int ILU_WARPS = ILU_THREADS / 32;
 constexpr int ILU_SPIN_LIMIT = 1 << 21;          // ~1-2 s of polling per wait
+#ifndef ILU_SPIN_HOT
+#define ILU_SPIN_HOT 256
+#endif
+// polls without sleeping before the back-off starts: an input usually
+// arrives within a few L2 round trips, and a sleeping warp wakes late
+constexpr int ILU_SPIN_HOT_POLLS = ILU_SPIN_HOT;
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p)
 {
@@ -66,7 +72,8 @@ __device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int *p)
 
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
-// Wait until *f == target (bounded): relaxed polls with exponential back-off.
+// Wait until *f == target (bounded): relaxed polls, the first ILU_SPIN_HOT_POLLS
+// back to back, then with exponential back-off.
 // The caller completes the acquire with fence_acq_rel_gpu() after the polls
 // of all its lanes (one fence per row instead of one acquire per input).
 // Returns false after a time-out, or when another warp has already timed out.
@@ -75,8 +82,10 @@ __device__ __forceinline__ bool wait_flag(const unsigned int *f, unsigned int ta
   if (ld_relaxed_u32(f) == target) return true;
   unsigned int ns = 32;
   for (int it = 0; it < ILU_SPIN_LIMIT; it++) {
-    __nanosleep(ns);
-    if (ns < 1024) ns <<= 1;
+    if (it >= ILU_SPIN_HOT_POLLS) {
+      __nanosleep(ns);
+      if (ns < 1024) ns <<= 1;
+    }
     if (ld_relaxed_u32(f) == target) return true;
     if (*(volatile unsigned int *)&ctl->error) return false;
   }
@@ -311,7 +320,7 @@ template <> struct Sentinel<float> {
   static __device__ __forceinline__ float sentinel() { return __uint_as_float(bits); }
 };
 
-// value at p once it is no longer the sentinel (bounded wait)
+// value at p once it is no longer the sentinel (bounded wait; polls as in wait_flag)
 template <typename VT>
 __device__ __forceinline__ double wait_value(const VT *p, typename Sentinel<VT>::U v, TriCtl *ctl)
 {
@@ -319,8 +328,10 @@ __device__ __forceinline__ double wait_value(const VT *p, typename Sentinel<VT>:
   if (v != S::bits) return (double)S::value(v);
   unsigned int ns = 32;
   for (int it = 0; it < ILU_SPIN_LIMIT; it++) {
-    __nanosleep(ns);
-    if (ns < 256) ns <<= 1;
+    if (it >= ILU_SPIN_HOT_POLLS) {
+      __nanosleep(ns);
+      if (ns < 256) ns <<= 1;
+    }
     v = S::load(p);
     if (v != S::bits) return (double)S::value(v);
     if (*(volatile unsigned int *)&ctl->error) break;
@@ -341,20 +352,31 @@ __global__ void fill_sentinel_f32(int64_t n, float *y)
     y[i] = Sentinel<float>::sentinel();
 }
 
-constexpr int TRSV_BATCH = 4;   // input loads in flight per lane
+constexpr int TRSV_BATCH = 4;        // input loads in flight per lane for blocks beyond the pipelined ones
 constexpr int TRSV_CHAIN_MAX = 128;
+constexpr int TRSV_ROW_BLOCKS = 14;  // blocks per row held in the pipeline registers (a 27-point row: 13)
 
 // One warp per chain of rows (see IluPattern::lchain / uchain), chains in
 // level order of the chain DAG.  The chain's rows are solved in order; inputs
 // from the chain itself come from shared memory, inputs from other chains
 // from global memory once they are no longer the sentinel.
 //
+// The rows of a chain run through a three-stage software pipeline, so that
+// the memory latencies of a row overlap the work of the row before it: while
+// row s is finished, the warp already holds the matrix values and the other
+// chains' input values of row s+1, the column indices of row s+2 are in
+// flight, and so is the block range of row s+3.  A lane holds PF blocks of a
+// row in registers (G blocks per warp pass, lanes g = lane / (NB*NB));
+// further blocks (fill rows of ILU(k), k >= 1) are loaded when their row is
+// finished.  Per lane the products are summed in block order, so the result
+// does not depend on how far ahead the loads ran.
+//
 // Lower:  y_i = r_P(i) - sum_{p<i} L_ip y_p
 // Upper:  z_P(i) = U_ii^-1 (y_i - sum_{p>i} U_ip z_P(p))
 // with P the factor's row order (perm; NULL: the identity): y is indexed by
 // factor row, r and z by node.
 template <int NB, bool UPPER, typename FT, typename VT>
-__global__ void __launch_bounds__(ILU_THREADS)
+__global__ void __launch_bounds__(ILU_THREADS, 2)
 ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restrict__ chains,
          const int32_t *__restrict__ fptr, const int32_t *__restrict__ fcol, const int32_t *__restrict__ fdiag,
          const FT *__restrict__ fval, const FT *__restrict__ fdinv, const int32_t *__restrict__ perm, const VT *r,
@@ -363,87 +385,202 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
   if (st && (!st->active || st->it != j)) return;
   if (active && !active[0]) return;
   using S = Sentinel<VT>;
+  using U = typename S::U;
   constexpr int BB = NB * NB;
   constexpr int G = 32 / BB;
+  constexpr int PF = (TRSV_ROW_BLOCKS + G - 1) / G;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   __shared__ double red[ILU_WARPS][32];
   __shared__ double sv[ILU_WARPS][NB];
   __shared__ double cache[ILU_WARPS][TRSV_CHAIN_MAX * NB];
   const unsigned int epoch = *(volatile unsigned int *)&ctl->epoch;
   const int g = lane / BB, e = lane % BB, ec = e % NB;
+  const bool glane = g < G;
   // the vector the off-diagonal products read: y (lower) or z (upper)
   const VT *src = UPPER ? z : y;
+  // position of column p in src: z is indexed by node, y by factor row
+  auto at = [&](int p) -> int64_t { return (int64_t)((UPPER && perm) ? perm[p] : p) * NB + ec; };
   while (true) {
     const int tk = draw_ticket(ctl, lane);
     if (tk >= nchains) break;
     const int c = order[tk];
     const int lo = chains[2 * c], hi = chains[2 * c + 1];
-    for (int step = 0; step < hi - lo; step++) {
-      const int i = UPPER ? hi - 1 - step : lo + step;
-      const int q0 = UPPER ? fdiag[i] + 1 : fptr[i];
-      const int q1 = UPPER ? fptr[i + 1] : fdiag[i];
-      // blocks in the order farthest column first, so the chain's own
-      // previous row (the input finished last) is consumed last
+    const int len = hi - lo;
+    auto row = [&](int s) { return UPPER ? hi - 1 - s : lo + s; };
+    auto own = [&](int p) { return UPPER ? p < hi : p >= lo; };
+    // strictly lower (upper) blocks [qa, qb) of the chain's s-th row; the
+    // qq-th block of a row is the farthest column first, so the chain's own
+    // previous row (the input finished last) is consumed last
+    auto range = [&](int s, int &qa, int &qb) {
+      qa = qb = 0;
+      if (s < len) {
+        const int i = row(s);
+        qa = UPPER ? fdiag[i] + 1 : fptr[i];
+        qb = UPPER ? fptr[i + 1] : fdiag[i];
+      }
+    };
+    auto blk = [&](int qa, int qb, int qq) { return UPPER ? qb - 1 - qq : qa + qq; };
+    auto cols = [&](int qa, int qb, int (&p)[PF]) {
+#pragma unroll
+      for (int k = 0; k < PF; k++) {
+        const int qq = k * G + g;
+        p[k] = (glane && qq < qb - qa) ? fcol[blk(qa, qb, qq)] : -1;
+      }
+    };
+    // matrix values, other chains' inputs and the row's own data (r_P(i) or
+    // y_i, and the row of U_ii^-1) of the s-th row
+    auto vals = [&](int s, int qa, int qb, const int (&p)[PF], FT (&a)[PF], U (&v)[PF], VT &b, FT (&d)[NB]) {
+#pragma unroll
+      for (int k = 0; k < PF; k++)
+        a[k] = p[k] >= 0 ? fval[(int64_t)blk(qa, qb, k * G + g) * BB + e] : FT(0);
+#pragma unroll
+      for (int k = 0; k < PF; k++) v[k] = (p[k] >= 0 && !own(p[k])) ? S::load(src + at(p[k])) : U(0);
+      b = VT(0);
+#pragma unroll
+      for (int cc = 0; cc < NB; cc++) d[cc] = FT(0);
+      if (s < len) {
+        const int i = row(s);
+        if constexpr (NB == 4) {
+          // every lane: entry er of the row's vector, entry (er, ec) of U_ii^-1
+          if (UPPER) {
+            b = y[(int64_t)i * NB + e / NB];
+            d[0] = fdinv[(int64_t)i * BB + e];
+          } else {
+            b = r[(int64_t)(perm ? perm[i] : i) * NB + e / NB];
+          }
+        } else if (lane < NB) {
+          if (UPPER) {
+            b = y[(int64_t)i * NB + lane];
+#pragma unroll
+            for (int cc = 0; cc < NB; cc++) d[cc] = fdinv[(int64_t)i * BB + lane * NB + cc];
+          } else {
+            b = r[(int64_t)(perm ? perm[i] : i) * NB + lane];
+          }
+        }
+      }
+    };
+
+    int qa0, qb0, qa1, qb1, qa2, qb2;
+    int p0[PF], p1[PF], p2[PF];
+    FT a0[PF], a1[PF], d0[NB], d1[NB];
+    U v0[PF], v1[PF];
+    VT b0, b1;
+    range(0, qa0, qb0);
+    range(1, qa1, qb1);
+    range(2, qa2, qb2);
+    cols(qa0, qb0, p0);
+    cols(qa1, qb1, p1);
+    vals(0, qa0, qb0, p0, a0, v0, b0, d0);
+    for (int s = 0; s < len; s++) {
+      const int i = row(s);
+      // loads for the rows ahead
+      vals(s + 1, qa1, qb1, p1, a1, v1, b1, d1);
+      cols(qa2, qb2, p2);
+      int qa3, qb3;
+      range(s + 3, qa3, qb3);
+
+      // row s: products in block order, other chains' inputs once they are
+      // no longer the sentinel, the chain's own from shared memory
       double acc = 0.0;
-      const int nq = q1 - q0;
-      for (int qb = 0; qb < nq; qb += G * TRSV_BATCH) {
-        typename S::U v[TRSV_BATCH];
+#pragma unroll
+      for (int k = 0; k < PF; k++) {
+        if (p0[k] < 0) continue;
+        const double xv = own(p0[k]) ? cache[w][(UPPER ? hi - 1 - p0[k] : p0[k] - lo) * NB + ec]
+                                     : wait_value<VT>(src + at(p0[k]), v0[k], ctl);
+        acc = fma((double)a0[k], xv, acc);
+      }
+      const int nq = qb0 - qa0;
+      for (int qb = G * PF; qb < nq; qb += G * TRSV_BATCH) {
+        U v[TRSV_BATCH];
         int p[TRSV_BATCH];
         double a[TRSV_BATCH];
-        bool own[TRSV_BATCH];
 #pragma unroll
         for (int k = 0; k < TRSV_BATCH; k++) {
           const int qq = qb + k * G + g;
-          const bool ok = (g < G && qq < nq);
-          const int q = UPPER ? q1 - 1 - qq : q0 + qq;
+          const bool ok = (glane && qq < nq);
+          const int q = blk(qa0, qb0, qq);
           p[k] = ok ? fcol[q] : -1;
           a[k] = ok ? (double)fval[(int64_t)q * BB + e] : 0.0;
-          own[k] = ok && (UPPER ? p[k] < hi : p[k] >= lo);
         }
-        // z is indexed by node, y by factor row
-        int64_t at[TRSV_BATCH];
 #pragma unroll
-        for (int k = 0; k < TRSV_BATCH; k++)
-          at[k] = (int64_t)((UPPER && perm && p[k] >= 0) ? perm[p[k]] : p[k]) * NB + ec;
-#pragma unroll
-        for (int k = 0; k < TRSV_BATCH; k++) v[k] = (p[k] >= 0 && !own[k]) ? S::load(src + at[k]) : 0;
+        for (int k = 0; k < TRSV_BATCH; k++) v[k] = (p[k] >= 0 && !own(p[k])) ? S::load(src + at(p[k])) : U(0);
 #pragma unroll
         for (int k = 0; k < TRSV_BATCH; k++) {
           if (p[k] < 0) continue;
-          const double xv = own[k] ? cache[w][(UPPER ? hi - 1 - p[k] : p[k] - lo) * NB + ec]
-                                   : wait_value<VT>(src + at[k], v[k], ctl);
+          const double xv = own(p[k]) ? cache[w][(UPPER ? hi - 1 - p[k] : p[k] - lo) * NB + ec]
+                                      : wait_value<VT>(src + at(p[k]), v[k], ctl);
           acc = fma(a[k], xv, acc);
         }
       }
+      const int64_t node = perm ? perm[i] : i;
+      if constexpr (NB == 4) {
+        // 4x4 blocks, two per warp pass: lane = 16 g + 4 er + ec.  Sum the
+        // products of block row er over ec (lane bits 0-1) and g (bit 4)
+        // with shuffles; every lane then holds entry er of the row's vector.
+        constexpr unsigned FULL = 0xffffffffu;
+        double t = acc;
+        t += __shfl_xor_sync(FULL, t, 1);
+        t += __shfl_xor_sync(FULL, t, 2);
+        t += __shfl_xor_sync(FULL, t, 16);
+        const double sr = (double)b0 - t;
+        const int er = e / NB;
+        if (UPPER) {
+          // z_i = U_ii^-1 s: lane (er, ec) forms (U_ii^-1)_{er,ec} s_ec, summed over ec
+          double x = (double)d0[0] * __shfl_sync(FULL, sr, ec * NB);
+          x += __shfl_xor_sync(FULL, x, 1);
+          x += __shfl_xor_sync(FULL, x, 2);
+          if (lane < BB && ec == 0) {
+            const VT vv = (VT)x;
+            cache[w][s * NB + er] = (double)vv;
+            S::store(z + node * NB + er, vv);
+            y[(int64_t)i * NB + er] = S::sentinel();
+          }
+        } else if (lane < BB && ec == 0) {
+          const VT vv = (VT)sr;
+          cache[w][s * NB + er] = (double)vv;
+          z[node * NB + er] = S::sentinel();
+          S::store(y + (int64_t)i * NB + er, vv);
+        }
+        __syncwarp();
+      } else {
       red[w][lane] = acc;
       __syncwarp();
-      const int64_t node = perm ? perm[i] : i;
       if (lane < NB) {
-        double s = UPPER ? (double)y[(int64_t)i * NB + lane] : (double)r[node * NB + lane];
+        double sum = (double)b0;
 #pragma unroll
         for (int gg = 0; gg < G; gg++)
 #pragma unroll
-          for (int cc = 0; cc < NB; cc++) s -= red[w][gg * BB + lane * NB + cc];
-        sv[w][lane] = s;
+          for (int cc = 0; cc < NB; cc++) sum -= red[w][gg * BB + lane * NB + cc];
+        sv[w][lane] = sum;
       }
       __syncwarp();
       if (lane < NB) {
         if (UPPER) {
-          double v = 0.0;
+          double x = 0.0;
 #pragma unroll
-          for (int cc = 0; cc < NB; cc++) v = fma((double)fdinv[(int64_t)i * BB + lane * NB + cc], sv[w][cc], v);
-          const VT vv = (VT)v;
-          cache[w][step * NB + lane] = (double)vv;
+          for (int cc = 0; cc < NB; cc++) x = fma((double)d0[cc], sv[w][cc], x);
+          const VT vv = (VT)x;
+          cache[w][s * NB + lane] = (double)vv;
           S::store(z + node * NB + lane, vv);
           y[(int64_t)i * NB + lane] = S::sentinel();
         } else {
           const VT vv = (VT)sv[w][lane];
-          cache[w][step * NB + lane] = (double)vv;
+          cache[w][s * NB + lane] = (double)vv;
           z[node * NB + lane] = S::sentinel();
           S::store(y + (int64_t)i * NB + lane, vv);
         }
       }
       __syncwarp();
+      }
+      // advance the pipeline
+      qa0 = qa1; qb0 = qb1; qa1 = qa2; qb1 = qb2; qa2 = qa3; qb2 = qb3;
+      b0 = b1;
+#pragma unroll
+      for (int k = 0; k < PF; k++) {
+        p0[k] = p1[k]; p1[k] = p2[k]; a0[k] = a1[k]; v0[k] = v1[k];
+      }
+#pragma unroll
+      for (int cc = 0; cc < NB; cc++) d0[cc] = d1[cc];
     }
   }
   launch_done(ctl, lane, epoch);

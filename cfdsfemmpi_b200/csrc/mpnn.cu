@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -79,6 +80,7 @@ struct cfdgpu_mpnn {
   float *lossbuf = nullptr;
   // normalisation
   float in_scale[8] = {1, 1, 1, 1, 1, 1, 1, 1}, out_scale[4] = {1, 1, 1, 1};
+  double3 xlo = {0.0, 0.0, 0.0}, xinv = {1.0, 1.0, 1.0};   // bounding box of the nodes: lower corner, 1 / extent
   // samples on the device: inputs (bf16 features), targets, masks
   std::vector<bf16 *> sx;
   std::vector<float *> st;
@@ -219,7 +221,7 @@ __global__ void k_mean_agg(int N, const int32_t *__restrict__ rowptr, const int3
 // input features of one sample / prediction
 __global__ void k_features(int N, int ndof, int ndim, const double *__restrict__ un, const double *__restrict__ unm1,
                            const double *__restrict__ coords, float s0, float s1, float s2, float s3, float d0,
-                           float d1, float d2, float d3, bf16 *__restrict__ X)
+                           float d1, float d2, float d3, double3 xlo, double3 xinv, bf16 *__restrict__ X)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -232,7 +234,9 @@ __global__ void k_features(int N, int ndof, int ndim, const double *__restrict__
     f[c] = (float)(u / su[c]);
     f[ndof + c] = (float)((u - um) / sd[c]);
   }
-  for (int c = 0; c < ndim; c++) f[2 * ndof + c] = (float)(2.0 * coords[(int64_t)i * ndim + c] - 1.0);
+  // coordinates mapped from the mesh's bounding box to [-1, 1] (2X - 1 on the unit square / cube)
+  const double lo[3] = {xlo.x, xlo.y, xlo.z}, inv[3] = {xinv.x, xinv.y, xinv.z};
+  for (int c = 0; c < ndim; c++) f[2 * ndof + c] = (float)(2.0 * ((coords[(int64_t)i * ndim + c] - lo[c]) * inv[c]) - 1.0);
 #pragma unroll
   for (int c = 0; c < FIN; c++) X[(int64_t)i * FIN + c] = __float2bfloat16(f[c]);
 }
@@ -513,7 +517,7 @@ int sample_features(cfdgpu_mpnn *m, const double *d_unm1, const double *d_un, bf
   k_features<<<(N + 255) / 256, 256, 0, m->g.stream>>>(N, m->g.ndof, m->g.ndim, d_un, d_unm1, m->g.coords,
                                                        m->in_scale[0], m->in_scale[1], m->in_scale[2],
                                                        m->in_scale[3], m->in_scale[4], m->in_scale[5],
-                                                       m->in_scale[6], m->in_scale[7], X);
+                                                       m->in_scale[6], m->in_scale[7], m->xlo, m->xinv, X);
   return cudaGetLastError() == cudaSuccess ? 0 : CFDGPU_ECUDA;
 }
 
@@ -577,6 +581,24 @@ int cfdgpu_mpnn_create(cfdgpu_handle *h, uint64_t seed, cfdgpu_mpnn **out)
     for (int i = 0; i < K * NO; i++) p[weight_off(m->L, w) + i] = a * uni(gen);
   }
   cudaMemcpy(m->P, p.data(), sizeof(float) * p.size(), cudaMemcpyHostToDevice);
+  {
+    std::vector<double> X((size_t)m->N * m->g.ndim);
+    if (cudaMemcpy(X.data(), m->g.coords, sizeof(double) * X.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      m->err = "coordinate copy failed";
+      return CFDGPU_ECUDA;
+    }
+    double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+    for (int c = 0; c < m->g.ndim; c++) {
+      lo[c] = hi[c] = X[c];
+      for (int i = 0; i < m->N; i++) {
+        lo[c] = std::min(lo[c], X[(size_t)i * m->g.ndim + c]);
+        hi[c] = std::max(hi[c], X[(size_t)i * m->g.ndim + c]);
+      }
+      if (!(hi[c] > lo[c])) hi[c] = lo[c] + 1.0;
+    }
+    m->xlo = make_double3(lo[0], lo[1], lo[2]);
+    m->xinv = make_double3(1.0 / (hi[0] - lo[0]), 1.0 / (hi[1] - lo[1]), 1.0 / (hi[2] - lo[2]));
+  }
   // activations
   if ((rc = dalloc(m, &m->X, (size_t)Np * FIN)) || (rc = dalloc(m, &m->Ze, (size_t)Np * HID)) ||
       (rc = dalloc(m, &m->H3b, (size_t)Np * HID)) || (rc = dalloc(m, &m->Y, (size_t)Np * FOUT)))

@@ -55,7 +55,9 @@ def features(u_nm1, u_n, coords, ndof, ndim, in_scale):
         f[:, c] = (un[:, c] / np.float64(np.float32(in_scale[c]))).astype(np.float32)
         f[:, ndof + c] = (du[:, c] / np.float64(np.float32(in_scale[ndof + c]))).astype(np.float32)
     for c in range(ndim):
-        f[:, 2 * ndof + c] = (2.0 * coords[:, c] - 1.0).astype(np.float32)
+        lo, hi = coords[:, c].min(), coords[:, c].max()
+        inv = 1.0 / (hi - lo) if hi > lo else 1.0
+        f[:, 2 * ndof + c] = (2.0 * ((coords[:, c] - lo) * inv) - 1.0).astype(np.float32)
     return bf16(f)
 
 
