@@ -122,15 +122,18 @@ def cylinder_ogrid(nt: int = 256, nr: int = 128, r_in: float = 0.5, r_out: float
     radial spacing starting at dr0.  Boundary conditions: no-slip on the
     cylinder, inflow (1, 0) on the outer arc where x < 0, traction-free
     (nothing prescribed) where x >= 0; no pressure pin (the free outflow fixes
-    the pressure level).  Nodes are numbered ring by ring (k outward), i
-    counter-clockwise from the +x axis."""
+    the pressure level).  Nodes are numbered ray by ray (i counter-clockwise
+    from the +x axis), k outward within a ray.  (Ring-by-ring numbering
+    would chain every row of an incomplete-LU factorisation in natural order
+    to the one before it through the ring's closure, a dependency depth of
+    the node count; ray by ray the depth is about nr + 2 nt.)"""
     q = _geometric_ratio(nr, r_in, r_out, dr0)
     r = r_in + dr0 * (q ** np.arange(nr + 1) - 1.0) / (q - 1.0)
     r[-1] = r_out
     th = 2.0 * np.pi * np.arange(nt) / nt
-    R, TH = np.meshgrid(r, th, indexing="ij")          # (nr+1, nt)
+    TH, R = np.meshgrid(th, r, indexing="ij")          # (nt, nr+1)
     coords = np.stack([(R * np.cos(TH)).ravel(), (R * np.sin(TH)).ravel()], axis=1)
-    nid = lambda i, k: (i % nt) + nt * k
+    nid = lambda i, k: k + (nr + 1) * (i % nt)
     kk, ii = np.meshgrid(np.arange(nr), np.arange(nt), indexing="ij")
     kk = kk.ravel(); ii = ii.ravel()
     # (radial, then tangential) edge order: counter-clockwise in (x, y)

@@ -199,21 +199,26 @@ def test_cylinder_ogrid_matches_its_description():
     """O-grid of the cylinder-wake configuration: 256 x 128 quads (33,024
     nodes), radial spacing 0.005 at r = 0.5 growing geometrically to r = 20,
     counter-clockwise elements, no-slip on the cylinder, inflow on the outer
-    arc where x < 0, nothing prescribed where x >= 0."""
+    arc where x < 0, nothing prescribed where x >= 0; nodes numbered ray by
+    ray (radial index fastest)."""
     m = meshgen.cylinder_ogrid()
     assert (m.nNode, m.nElem) == (33024, 32768)
-    r = np.hypot(m.coords[:, 0], m.coords[:, 1]).reshape(129, 256)
-    assert np.allclose(r[0], 0.5) and np.allclose(r[-1], 20.0)
-    assert abs((r[1, 0] - r[0, 0]) - 0.005) < 1e-12
-    dr = np.diff(r[:, 0])
+    r = np.hypot(m.coords[:, 0], m.coords[:, 1]).reshape(256, 129)
+    assert np.allclose(r[:, 0], 0.5) and np.allclose(r[:, -1], 20.0)
+    assert abs((r[0, 1] - r[0, 0]) - 0.005) < 1e-12
+    dr = np.diff(r[0])
     assert np.allclose(dr[1:] / dr[:-1], dr[1] / dr[0])
+    th = np.arctan2(m.coords[:, 1], m.coords[:, 0]).reshape(256, 129)
+    assert np.allclose(th[:, 0], th[:, -1]) and np.all(np.diff(np.unwrap(th[:, 0])) > 0)
     p = m.coords[m.conn]
     area2 = (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 3, 1] - p[:, 1, 1]) - (p[:, 2, 1] - p[:, 0, 1]) * (p[:, 3, 0] - p[:, 1, 0])
     assert np.all(area2 > 0)
     d = m.dbc
-    cyl = d[d[:, 0] < 256]
+    on_cyl = d[:, 0].astype(int) % 129 == 0
+    cyl = d[on_cyl]
     assert len(cyl) == 512 and np.all(cyl[:, 2] == 0.0)
-    outer = d[d[:, 0] >= 256]
+    outer = d[~on_cyl]
+    assert np.all(outer[:, 0].astype(int) % 129 == 128)
     assert np.all(m.coords[outer[:, 0].astype(int), 0] < 0)
     assert np.all(outer[outer[:, 1] == 0, 2] == 1.0) and np.all(outer[outer[:, 1] == 1, 2] == 0.0)
     assert not np.any(d[:, 1] == 2)

@@ -5,12 +5,14 @@ input/cylinder2d-blockmesh-Re100-GA2-rho0p0-dt0p1-SI.dat (12,675 nodes,
 iterative option files, input/petsc_options_bcgs.dat (BiCGStab) and
 input/petsc_options_gmres.dat (GMRES(20)), both with block Jacobi and ILU(3)
 sub-solves.  The reference ships no solution for this case, so the GPU run is
-compared with the oracle running the same solver from rest: fields after the
-first steps to max(1e-8, 2 x the oracle's own spread between one and eight
-host threads) relative L2, and Krylov counts within max(3, 5 %, 2 x the oracle's
-own spread) from the second step on.  BiCGStab's count on the first step from
-rest moves by a third with the summation order alone (338 against 266 its in
-two oracle runs), so there it only has to stay within a factor of two.
+compared with the oracle running the same solver from rest on one host thread
+(OpenMP reductions combine in no fixed order, and BiCGStab's first solve from
+rest is chaotic: four oracle runs on eight threads took 306, 325 and 442
+iterations, the last ending in a breakdown, one thread 503).  Fields after the
+first steps agree to max(1e-8, 2 x the distance between the oracle's
+BiCGStab and GMRES answers), which measures how far rtol 1e-10 determines the
+solution.  GMRES counts agree within max(3, 5 %) on every solve; BiCGStab's
+within a factor of two on the first solve and max(3, 10 %) after it.
 """
 import gzip
 import os
@@ -53,24 +55,22 @@ def test_reference_cylinder_with_its_option_files(golden_dir, tmp_path, options)
     kw = fem.solver_kw
     fem.deallocatePetscObjects()
 
-    okw = dict(solver=kw["ksp"], rtol=kw["rtol"], max_it=kw["max_it"], pc="bjacobi", ilu_levels=kw["ilu_levels"],
-               bjacobi_blocks=kw["bjacobi_blocks"])
-    if kw["ksp"] == "gmres":
-        okw["restart"] = kw["restart"]
-    runs = {}
-    # fixed thread counts, so the oracle's summation orders do not depend on
-    # the machine (BiCGStab's first solve from rest is sensitive to them)
-    for threads in (8, 1):
-        ref = oracle.OracleFEM(fem.mesh, fem.ctrl, threads=threads, **okw)
+    def run_oracle(ksp):
+        okw = dict(solver=ksp, rtol=kw["rtol"], max_it=kw["max_it"], pc="bjacobi", ilu_levels=kw["ilu_levels"],
+                   bjacobi_blocks=kw["bjacobi_blocks"], restart=20, threads=1)
+        ref = oracle.OracleFEM(fem.mesh, fem.ctrl, **okw)
         ref.solve(STEPS)
-        runs[threads] = (ref.solution(), [st["gmres_its"] for st in ref.stats])
-    (s_all, its_all), (s_one, its_one) = runs[max(runs)], runs[1]
-    spread = _rel(s_one, s_all)
-    err = _rel(s_gpu, s_all)
+        return ref.solution(), [st["gmres_its"] for st in ref.stats]
+
+    s_ref, its_ref = run_oracle(kw["ksp"])
+    s_other, _ = run_oracle("gmres" if kw["ksp"] == "bcgs" else "bcgs")
+    spread = _rel(s_other, s_ref)
+    err = _rel(s_gpu, s_ref)
     assert err <= max(1e-8, 2.0 * spread), (err, spread)
-    assert [len(a) for a in its_gpu] == [len(b) for b in its_all] == [len(c) for c in its_one]
-    rec = (its_gpu, its_all, its_one)
-    assert all(0.5 * y <= x <= 2.0 * y for x, y in zip(its_gpu[0], its_all[0])), rec
-    for a, b, c in zip(its_gpu[1:], its_all[1:], its_one[1:]):
-        for x, y, y1 in zip(a, b, c):
-            assert abs(x - y) <= max(3, 0.05 * y, 2 * abs(y1 - y)), rec
+    assert [len(a) for a in its_gpu] == [len(b) for b in its_ref]
+    rec = (its_gpu, its_ref)
+    if kw["ksp"] == "gmres":
+        assert all(abs(x - y) <= max(3, 0.05 * y) for a, b in zip(its_gpu, its_ref) for x, y in zip(a, b)), rec
+    else:
+        assert all(0.5 * y <= x <= 2.0 * y for x, y in zip(its_gpu[0], its_ref[0])), rec
+        assert all(abs(x - y) <= max(3, 0.1 * y) for a, b in zip(its_gpu[1:], its_ref[1:]) for x, y in zip(a, b)), rec
