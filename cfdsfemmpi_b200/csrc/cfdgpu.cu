@@ -497,29 +497,6 @@ static int ilu_factor_run32(cfdgpu_handle *h)
   return check_launch(h, "ilu_factor32");
 }
 
-// the triangular solves take more than the default 48 KB of dynamic shared
-// memory (their ring of factor values); set once per process
-static int trsv_prepare()
-{
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
-  std::call_once(once, [] {
-    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t e[8] = {
-        cudaFuncSetAttribute(ilu_trsv<4, false, double, double>, a, (int)trsv_smem_bytes<4, double>()),
-        cudaFuncSetAttribute(ilu_trsv<4, true, double, double>, a, (int)trsv_smem_bytes<4, double>()),
-        cudaFuncSetAttribute(ilu_trsv<3, false, double, double>, a, (int)trsv_smem_bytes<3, double>()),
-        cudaFuncSetAttribute(ilu_trsv<3, true, double, double>, a, (int)trsv_smem_bytes<3, double>()),
-        cudaFuncSetAttribute(ilu_trsv<4, false, float, float>, a, (int)trsv_smem_bytes<4, float>()),
-        cudaFuncSetAttribute(ilu_trsv<4, true, float, float>, a, (int)trsv_smem_bytes<4, float>()),
-        cudaFuncSetAttribute(ilu_trsv<3, false, float, float>, a, (int)trsv_smem_bytes<3, float>()),
-        cudaFuncSetAttribute(ilu_trsv<3, true, float, float>, a, (int)trsv_smem_bytes<3, float>())};
-    for (cudaError_t x : e)
-      if (x != cudaSuccess && err == cudaSuccess) err = x;
-  });
-  return err == cudaSuccess ? 0 : CFDGPU_ECUDA;
-}
-
 // z = (L U)^-1 r with the FP32 factors on FP32 vectors
 static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresState *st, int j, const int *active)
 {
@@ -529,12 +506,10 @@ static int ilu_apply32(cfdgpu_handle *h, const float *r, float *z, const GmresSt
   // every chain of a wavefront band is in flight at once: up to one warp per chain
   const int gl = ilu_grid(nl, nl), gu = ilu_grid(nu, nu);
 #define TRSV32(NB)                                                                                              \
-  ilu_trsv<NB, false, float, float><<<gl, ILU_THREADS, trsv_smem_bytes<NB, float>(), h->stream>>>(nl, h->flchord,  \
-      h->flchain, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, h->fperm, r, h->ybuf32, z, h->tctl, st, j,       \
-      active);                                                                                                    \
-  ilu_trsv<NB, true, float, float><<<gu, ILU_THREADS, trsv_smem_bytes<NB, float>(), h->stream>>>(nu, h->fuchord,   \
-      h->fuchain, h->frow, h->fcol, h->fdiag, h->fval32, h->fdinv32, h->fperm, nullptr, h->ybuf32, z, h->tctl, st, j, \
-      active);
+  ilu_trsv<NB, false, float, float><<<gl, ILU_THREADS, 0, h->stream>>>(nl, h->flchord, h->flchain, h->frow,       \
+      h->fcol, h->fdiag, h->fval32, h->fdinv32, h->fperm, r, h->ybuf32, z, h->tctl, st, j, active);                      \
+  ilu_trsv<NB, true, float, float><<<gu, ILU_THREADS, 0, h->stream>>>(nu, h->fuchord, h->fuchain, h->frow,        \
+      h->fcol, h->fdiag, h->fval32, h->fdinv32, h->fperm, nullptr, h->ybuf32, z, h->tctl, st, j, active);
   if (h->ndof == 4) { TRSV32(4); } else { TRSV32(3); }
 #undef TRSV32
   prof_end(h, pi);
@@ -569,10 +544,10 @@ static int ilu_apply(cfdgpu_handle *h, const double *r, double *z, const GmresSt
   // every chain of a wavefront band is in flight at once: up to one warp per chain
   const int gl = ilu_grid(nl, nl), gu = ilu_grid(nu, nu);
 #define TRSV64(NB)                                                                                                \
-  ilu_trsv<NB, false, double, double><<<gl, ILU_THREADS, trsv_smem_bytes<NB, double>(), h->stream>>>(nl, h->flchord,  \
-      h->flchain, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, h->fperm, r, h->ybuf, z, h->tctl, st, j, active);     \
-  ilu_trsv<NB, true, double, double><<<gu, ILU_THREADS, trsv_smem_bytes<NB, double>(), h->stream>>>(nu, h->fuchord,   \
-      h->fuchain, h->frow, h->fcol, h->fdiag, h->fval, h->fdinv, h->fperm, nullptr, h->ybuf, z, h->tctl, st, j, active);
+  ilu_trsv<NB, false, double, double><<<gl, ILU_THREADS, 0, h->stream>>>(nl, h->flchord, h->flchain, h->frow,       \
+      h->fcol, h->fdiag, h->fval, h->fdinv, h->fperm, r, h->ybuf, z, h->tctl, st, j, active);                              \
+  ilu_trsv<NB, true, double, double><<<gu, ILU_THREADS, 0, h->stream>>>(nu, h->fuchord, h->fuchain, h->frow,        \
+      h->fcol, h->fdiag, h->fval, h->fdinv, h->fperm, nullptr, h->ybuf, z, h->tctl, st, j, active);
   if (h->ndof == 4) { TRSV64(4); } else { TRSV64(3); }
 #undef TRSV64
   prof_end(h, pi);
@@ -1345,10 +1320,6 @@ int cfdgpu_create(const cfdgpu_mesh *mesh, const cfdgpu_control *ctrl, const cfd
       CK(cudaMemset(h->fval, 0, sizeof(double) * f.nnzb() * bb));
       if ((rc = dalloc(h, &h->fdinv, (size_t)h->nNode * bb))) return rc;
       CK(cudaMemset(h->fdinv, 0, sizeof(double) * h->nNode * bb));
-    }
-    if ((rc = trsv_prepare())) {
-      h->err = "cannot raise the triangular solves' shared-memory limit";
-      return rc;
     }
     if ((rc = dalloc(h, &h->iflags, (size_t)h->nNode))) return rc;
     CK(cudaMemset(h->iflags, 0, sizeof(unsigned int) * h->nNode));

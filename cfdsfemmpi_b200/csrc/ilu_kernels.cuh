@@ -354,51 +354,19 @@ __global__ void fill_sentinel_f32(int64_t n, float *y)
 
 constexpr int TRSV_BATCH = 4;        // input loads in flight per lane for blocks beyond the pipelined ones
 constexpr int TRSV_CHAIN_MAX = 128;
-constexpr int TRSV_ROW_BLOCKS = 14;  // blocks per row held in the pipeline (a 27-point row: 13)
-constexpr int TRSV_RING = 4;         // rows of factor values in flight per warp (shared-memory ring)
-
-template <int NB> struct TrsvShape {
-  static constexpr int BB = NB * NB;
-  static constexpr int G = 32 / BB;                                // blocks per warp pass
-  static constexpr int PF = (TRSV_ROW_BLOCKS + G - 1) / G;         // pipelined blocks per lane and row
-};
-
-// dynamic shared memory of ilu_trsv: per warp the chain's own results
-// (doubles) and the ring of factor values (PF blocks and one entry of U_ii^-1
-// per lane and row)
-template <int NB, typename FT>
-constexpr size_t trsv_smem_bytes()
-{
-  return (size_t)ILU_WARPS * (TRSV_CHAIN_MAX * NB * sizeof(double) +
-                              (size_t)TRSV_RING * (TrsvShape<NB>::PF + 1) * 32 * sizeof(FT));
-}
-
-__device__ __forceinline__ void cp_async_elem(void *smem, const double *g)
-{
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_elem(void *smem, const float *g)
-{
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(g)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+constexpr int TRSV_ROW_BLOCKS = 14;  // blocks per row held in the pipeline registers (a 27-point row: 13)
 
 // One warp per chain of rows (see IluPattern::lchain / uchain), chains in
 // level order of the chain DAG.  The chain's rows are solved in order; inputs
 // from the chain itself come from shared memory, inputs from other chains
 // from global memory once they are no longer the sentinel.
 //
-// The rows of a chain run through a software pipeline, so that the memory
-// latencies of a row overlap the work of the rows before it.  While row s is
-// finished, the factor values of rows s+1..s+3 are on their way into a
-// shared-memory ring (asynchronous copies, each lane copying the entries it
-// multiplies), the other chains' inputs of row s+1 and the column indices of
-// row s+2 are in flight, and so is the block range of row s+4.  A lane works
-// on PF blocks of a row (G blocks per warp pass, lanes g = lane / (NB*NB));
+// The rows of a chain run through a three-stage software pipeline, so that
+// the memory latencies of a row overlap the work of the row before it: while
+// row s is finished, the warp already holds the matrix values and the other
+// chains' input values of row s+1, the column indices of row s+2 are in
+// flight, and so is the block range of row s+3.  A lane holds PF blocks of a
+// row in registers (G blocks per warp pass, lanes g = lane / (NB*NB));
 // further blocks (fill rows of ILU(k), k >= 1) are loaded when their row is
 // finished.  Per lane the products are summed in block order, so the result
 // does not depend on how far ahead the loads ran.
@@ -406,8 +374,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // Lower:  y_i = r_P(i) - sum_{p<i} L_ip y_p
 // Upper:  z_P(i) = U_ii^-1 (y_i - sum_{p>i} U_ip z_P(p))
 // with P the factor's row order (perm; NULL: the identity): y is indexed by
-// factor row, r and z by node.  Launched with trsv_smem_bytes<NB, FT>() of
-// dynamic shared memory.
+// factor row, r and z by node.
 template <int NB, bool UPPER, typename FT, typename VT>
 __global__ void __launch_bounds__(ILU_THREADS, 2)
 ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restrict__ chains,
@@ -419,17 +386,13 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
   if (active && !active[0]) return;
   using S = Sentinel<VT>;
   using U = typename S::U;
-  constexpr int BB = TrsvShape<NB>::BB;
-  constexpr int G = TrsvShape<NB>::G;
-  constexpr int PF = TrsvShape<NB>::PF;
-  constexpr int RW = (PF + 1) * 32;                  // ring entries per row and warp
+  constexpr int BB = NB * NB;
+  constexpr int G = 32 / BB;
+  constexpr int PF = (TRSV_ROW_BLOCKS + G - 1) / G;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  extern __shared__ __align__(16) unsigned char trsv_smem[];
-  double *cache = reinterpret_cast<double *>(trsv_smem) + (size_t)w * TRSV_CHAIN_MAX * NB;
-  FT *ring = reinterpret_cast<FT *>(reinterpret_cast<double *>(trsv_smem) + (size_t)ILU_WARPS * TRSV_CHAIN_MAX * NB) +
-             (size_t)w * TRSV_RING * RW;
   __shared__ double red[ILU_WARPS][32];
   __shared__ double sv[ILU_WARPS][NB];
+  __shared__ double cache[ILU_WARPS][TRSV_CHAIN_MAX * NB];
   const unsigned int epoch = *(volatile unsigned int *)&ctl->epoch;
   const int g = lane / BB, e = lane % BB, ec = e % NB;
   const bool glane = g < G;
@@ -457,23 +420,6 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
       }
     };
     auto blk = [&](int qa, int qb, int qq) { return UPPER ? qb - 1 - qq : qa + qq; };
-    // factor values of the s-th row into ring slot s % TRSV_RING (one commit
-    // group per row, empty past the chain's end)
-    auto copy_row = [&](int s, int qa, int qb) {
-      FT *slot = ring + (s % TRSV_RING) * RW;
-      if (s < len) {
-#pragma unroll
-        for (int k = 0; k < PF; k++) {
-          const int qq = k * G + g;
-          if (glane && qq < qb - qa) cp_async_elem(slot + k * 32 + lane, fval + (int64_t)blk(qa, qb, qq) * BB + e);
-        }
-        // one entry of U_ii^-1 per lane (every lane for 4x4 blocks, each
-        // reading its own copy; lanes < BB for 3x3 blocks, read after a
-        // __syncwarp)
-        if (UPPER && (NB == 4 || lane < BB)) cp_async_elem(slot + PF * 32 + lane, fdinv + (int64_t)row(s) * BB + e);
-      }
-      cp_async_commit();
-    };
     auto cols = [&](int qa, int qb, int (&p)[PF]) {
 #pragma unroll
       for (int k = 0; k < PF; k++) {
@@ -481,46 +427,57 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
         p[k] = (glane && qq < qb - qa) ? fcol[blk(qa, qb, qq)] : -1;
       }
     };
-    // other chains' inputs and the row's own vector entry (r_P(i) or y_i) of
-    // the s-th row
-    auto inputs = [&](int s, const int (&p)[PF], U (&v)[PF], VT &b) {
+    // matrix values, other chains' inputs and the row's own data (r_P(i) or
+    // y_i, and the row of U_ii^-1) of the s-th row
+    auto vals = [&](int s, int qa, int qb, const int (&p)[PF], FT (&a)[PF], U (&v)[PF], VT &b, FT (&d)[NB]) {
+#pragma unroll
+      for (int k = 0; k < PF; k++)
+        a[k] = p[k] >= 0 ? fval[(int64_t)blk(qa, qb, k * G + g) * BB + e] : FT(0);
 #pragma unroll
       for (int k = 0; k < PF; k++) v[k] = (p[k] >= 0 && !own(p[k])) ? S::load(src + at(p[k])) : U(0);
       b = VT(0);
+#pragma unroll
+      for (int cc = 0; cc < NB; cc++) d[cc] = FT(0);
       if (s < len) {
         const int i = row(s);
-        // NB == 4: every lane holds entry er = e / NB; otherwise lanes < NB
-        const int rr = (NB == 4) ? e / NB : lane;
-        if (NB == 4 || lane < NB)
-          b = UPPER ? y[(int64_t)i * NB + rr] : r[(int64_t)(perm ? perm[i] : i) * NB + rr];
+        if constexpr (NB == 4) {
+          // every lane: entry er of the row's vector, entry (er, ec) of U_ii^-1
+          if (UPPER) {
+            b = y[(int64_t)i * NB + e / NB];
+            d[0] = fdinv[(int64_t)i * BB + e];
+          } else {
+            b = r[(int64_t)(perm ? perm[i] : i) * NB + e / NB];
+          }
+        } else if (lane < NB) {
+          if (UPPER) {
+            b = y[(int64_t)i * NB + lane];
+#pragma unroll
+            for (int cc = 0; cc < NB; cc++) d[cc] = fdinv[(int64_t)i * BB + lane * NB + cc];
+          } else {
+            b = r[(int64_t)(perm ? perm[i] : i) * NB + lane];
+          }
+        }
       }
     };
 
-    int qa0, qb0, qa1, qb1, qa2, qb2, qa3, qb3;
+    int qa0, qb0, qa1, qb1, qa2, qb2;
     int p0[PF], p1[PF], p2[PF];
+    FT a0[PF], a1[PF], d0[NB], d1[NB];
     U v0[PF], v1[PF];
     VT b0, b1;
     range(0, qa0, qb0);
     range(1, qa1, qb1);
     range(2, qa2, qb2);
-    range(3, qa3, qb3);
-    copy_row(0, qa0, qb0);
-    copy_row(1, qa1, qb1);
-    copy_row(2, qa2, qb2);
     cols(qa0, qb0, p0);
     cols(qa1, qb1, p1);
-    inputs(0, p0, v0, b0);
+    vals(0, qa0, qb0, p0, a0, v0, b0, d0);
     for (int s = 0; s < len; s++) {
       const int i = row(s);
       // loads for the rows ahead
-      int qa4, qb4;
-      range(s + 4, qa4, qb4);
-      copy_row(s + 3, qa3, qb3);
+      vals(s + 1, qa1, qb1, p1, a1, v1, b1, d1);
       cols(qa2, qb2, p2);
-      inputs(s + 1, p1, v1, b1);
-      // row s's copies have landed once at most the three later groups are pending
-      cp_async_wait<TRSV_RING - 1>();
-      const FT *a0 = ring + (s % TRSV_RING) * RW;
+      int qa3, qb3;
+      range(s + 3, qa3, qb3);
 
       // row s: products in block order, other chains' inputs once they are
       // no longer the sentinel, the chain's own from shared memory
@@ -528,9 +485,9 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
 #pragma unroll
       for (int k = 0; k < PF; k++) {
         if (p0[k] < 0) continue;
-        const double xv = own(p0[k]) ? cache[(UPPER ? hi - 1 - p0[k] : p0[k] - lo) * NB + ec]
+        const double xv = own(p0[k]) ? cache[w][(UPPER ? hi - 1 - p0[k] : p0[k] - lo) * NB + ec]
                                      : wait_value<VT>(src + at(p0[k]), v0[k], ctl);
-        acc = fma((double)a0[k * 32 + lane], xv, acc);
+        acc = fma((double)a0[k], xv, acc);
       }
       const int nq = qb0 - qa0;
       for (int qb = G * PF; qb < nq; qb += G * TRSV_BATCH) {
@@ -550,7 +507,7 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
 #pragma unroll
         for (int k = 0; k < TRSV_BATCH; k++) {
           if (p[k] < 0) continue;
-          const double xv = own(p[k]) ? cache[(UPPER ? hi - 1 - p[k] : p[k] - lo) * NB + ec]
+          const double xv = own(p[k]) ? cache[w][(UPPER ? hi - 1 - p[k] : p[k] - lo) * NB + ec]
                                       : wait_value<VT>(src + at(p[k]), v[k], ctl);
           acc = fma(a[k], xv, acc);
         }
@@ -569,63 +526,62 @@ ilu_trsv(int nchains, const int32_t *__restrict__ order, const int32_t *__restri
         const int er = e / NB;
         if (UPPER) {
           // z_i = U_ii^-1 s: lane (er, ec) forms (U_ii^-1)_{er,ec} s_ec, summed over ec
-          double x = (double)a0[PF * 32 + lane] * __shfl_sync(FULL, sr, ec * NB);
+          double x = (double)d0[0] * __shfl_sync(FULL, sr, ec * NB);
           x += __shfl_xor_sync(FULL, x, 1);
           x += __shfl_xor_sync(FULL, x, 2);
           if (lane < BB && ec == 0) {
             const VT vv = (VT)x;
-            cache[s * NB + er] = (double)vv;
+            cache[w][s * NB + er] = (double)vv;
             S::store(z + node * NB + er, vv);
             y[(int64_t)i * NB + er] = S::sentinel();
           }
         } else if (lane < BB && ec == 0) {
           const VT vv = (VT)sr;
-          cache[s * NB + er] = (double)vv;
+          cache[w][s * NB + er] = (double)vv;
           z[node * NB + er] = S::sentinel();
           S::store(y + (int64_t)i * NB + er, vv);
         }
         __syncwarp();
       } else {
-        red[w][lane] = acc;
-        __syncwarp();
-        if (lane < NB) {
-          double sum = (double)b0;
+      red[w][lane] = acc;
+      __syncwarp();
+      if (lane < NB) {
+        double sum = (double)b0;
 #pragma unroll
-          for (int gg = 0; gg < G; gg++)
+        for (int gg = 0; gg < G; gg++)
 #pragma unroll
-            for (int cc = 0; cc < NB; cc++) sum -= red[w][gg * BB + lane * NB + cc];
-          sv[w][lane] = sum;
+          for (int cc = 0; cc < NB; cc++) sum -= red[w][gg * BB + lane * NB + cc];
+        sv[w][lane] = sum;
+      }
+      __syncwarp();
+      if (lane < NB) {
+        if (UPPER) {
+          double x = 0.0;
+#pragma unroll
+          for (int cc = 0; cc < NB; cc++) x = fma((double)d0[cc], sv[w][cc], x);
+          const VT vv = (VT)x;
+          cache[w][s * NB + lane] = (double)vv;
+          S::store(z + node * NB + lane, vv);
+          y[(int64_t)i * NB + lane] = S::sentinel();
+        } else {
+          const VT vv = (VT)sv[w][lane];
+          cache[w][s * NB + lane] = (double)vv;
+          z[node * NB + lane] = S::sentinel();
+          S::store(y + (int64_t)i * NB + lane, vv);
         }
-        __syncwarp();
-        if (lane < NB) {
-          if (UPPER) {
-            double x = 0.0;
-#pragma unroll
-            for (int cc = 0; cc < NB; cc++) x = fma((double)a0[PF * 32 + lane * NB + cc], sv[w][cc], x);
-            const VT vv = (VT)x;
-            cache[s * NB + lane] = (double)vv;
-            S::store(z + node * NB + lane, vv);
-            y[(int64_t)i * NB + lane] = S::sentinel();
-          } else {
-            const VT vv = (VT)sv[w][lane];
-            cache[s * NB + lane] = (double)vv;
-            z[node * NB + lane] = S::sentinel();
-            S::store(y + (int64_t)i * NB + lane, vv);
-          }
-        }
-        __syncwarp();
+      }
+      __syncwarp();
       }
       // advance the pipeline
-      qa0 = qa1; qb0 = qb1; qa1 = qa2; qb1 = qb2; qa2 = qa3; qb2 = qb3; qa3 = qa4; qb3 = qb4;
+      qa0 = qa1; qb0 = qb1; qa1 = qa2; qb1 = qb2; qa2 = qa3; qb2 = qb3;
       b0 = b1;
 #pragma unroll
       for (int k = 0; k < PF; k++) {
-        p0[k] = p1[k]; p1[k] = p2[k]; v0[k] = v1[k];
+        p0[k] = p1[k]; p1[k] = p2[k]; a0[k] = a1[k]; v0[k] = v1[k];
       }
+#pragma unroll
+      for (int cc = 0; cc < NB; cc++) d0[cc] = d1[cc];
     }
-    // no copy of this chain may land in the ring after the next chain's
-    cp_async_wait<0>();
-    __syncwarp();
   }
   launch_done(ctl, lane, epoch);
 }
