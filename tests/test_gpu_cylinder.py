@@ -74,3 +74,52 @@ def test_reference_cylinder_with_its_option_files(golden_dir, tmp_path, options)
     else:
         assert all(0.5 * y <= x <= 2.0 * y for x, y in zip(its_gpu[0], its_ref[0])), rec
         assert all(abs(x - y) <= max(3, 0.1 * y) for a, b in zip(its_gpu[1:], its_ref[1:]) for x, y in zip(a, b)), rec
+
+
+def test_learned_guess_on_the_cylinder_wake():
+    """The learned-guess configuration's O-grid (256 x 128 quads, Re 100,
+    dt 0.1, seeded perturbation) with the reference's BiCGStab + ILU(3):
+    the network trained on steps 12..24 of the plain solve (after the inflow
+    ramp) predicts steps 25..28, which it has not seen.  Every held-out step
+    takes the guess, whose iteration-0 residual is below the constant
+    predictor's, and the fields stay those of the plain run (velocity to
+    1e-6: each solve stops at rtol 1e-10 relative to its own start)."""
+    from cfdsfemmpi_b200 import Handle, meshgen
+    from cfdsfemmpi_b200.surrogate import train_guess
+    mesh = meshgen.cylinder_ogrid()
+    ctrl = meshgen.control_for(40, 0.1, 0.01)
+    kw = dict(ksp="bcgs", pc="bjacobi", ilu_levels=3, rtol=1e-10, max_it=10000)
+    u0 = meshgen.cylinder_initial_state(mesh)
+    h0 = Handle(mesh, ctrl, **kw)
+    h0.set_solution(u0)
+    traj = [u0]
+    t = ctrl.dt
+    for _ in range(24):
+        assert h0.step(t, min(t, 1.0)).as_dict()["converged"]
+        traj.append(h0.get_solution())
+        t = t + ctrl.dt
+    prev, dot = h0.get_history()
+    h0.close()
+    out = {}
+    for mode in (None, ("network",)):
+        h = Handle(mesh, ctrl, **kw)
+        h.set_solution(traj[-1])
+        h.set_history(prev, dot)
+        net = None
+        if mode:
+            net, losses = train_guess(h, traj, iters=1500, lr=2e-3, seed=0, first=12)
+            assert losses[-1] < losses[0]
+            net.attach(mode)
+        tt, st = t, []
+        for _ in range(4):
+            st.append(h.step(tt, min(tt, 1.0)).as_dict())
+            tt = tt + ctrl.dt
+        out[mode] = (h.get_solution().reshape(-1, 3), st)
+        if net is not None:
+            net.close()
+        h.close()
+    (base, base_st), (guess, guess_st) = out[None], out[("network",)]
+    assert all(s["converged"] for s in guess_st)
+    assert all(s["guess_used"] and s["guess_norm"] < s["plain_norm"] for s in guess_st), guess_st
+    rel = np.linalg.norm(guess[:, :2] - base[:, :2]) / np.linalg.norm(base[:, :2])
+    assert rel < 1e-6, rel
