@@ -108,6 +108,8 @@ def parse():
     p.add_argument("--kernel-its", type=int, default=40,
                    help="kernels: GMRES iterations of the bounded profiling case")
     p.add_argument("--no-batch-mixed", action="store_true", help="batch: skip the mixed-precision batch arm")
+    p.add_argument("--no-batch-learned", action="store_true",
+                   help="batch: skip the arm with the shared, Re-conditioned guess network")
     p.add_argument("--batch-schedule", default="auto",
                    help="batch: 'auto' (autotune during the warm-up steps) or 'C,K,D' (concurrency, chunk, depth)")
     a = p.parse_args()
@@ -966,6 +968,62 @@ def run_batch(args, world, rank, local):
               "latency_ms": {"p50": float(np.percentile(lat_x, 50)), "p99": float(np.percentile(lat_x, 99))},
               "gmres_iters": int(its_x), "max_velocity_rel_diff_vs_constant_predictor": max(dvx)}
 
+    # the same batch with one guess network shared by every instance and
+    # conditioned on its Reynolds number (input channel log Re / log 5000):
+    # trained on the warm-up steps' samples of all instances (each on its own
+    # mesh), then each instance's network (the shared weights, its own
+    # condition) combined with the extrapolated increment by the min-residual
+    # rule, on the same timed steps
+    learned = None
+    if not args.no_batch_learned:
+        from cfdsfemmpi_b200.surrogate import attach_shared, train_shared
+        bl = Batch(pairs, **BATCH_SOLVER)
+        bl.set_schedule(0, 0, 0)
+        trajs = [[h.get_solution()] for h in bl.handles]
+        for k in range(warm):
+            bl.step(times(k))
+            for i, h in enumerate(bl.handles):
+                trajs[i].append(h.get_solution())
+        conds = [float(np.log(re) / np.log(5000.0)) for _, _, _, re in cases]
+        torch.cuda.synchronize()
+        T1 = time.perf_counter()
+        net0, shared, losses = train_shared(bl.handles, trajs, conds, iters=args.train_iters, lr=2e-3, seed=0,
+                                            first=2)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - T1
+        nsamples = net0.num_samples
+        net0.close()
+        nets = [attach_shared(h, shared, c) for h, c in zip(bl.handles, conds)]
+        del trajs
+        torch.cuda.synchronize()
+        T0 = time.perf_counter()
+        lat_l, its_l, used, ratios = [], 0, 0, []
+        for k in range(warm, warm + steps):
+            st, lat = bl.step(times(k))
+            lat_l.extend(lat.tolist())
+            its_l += sum(sum(s.ksp_its[:s.newton_iters]) for s in st)
+            for s_ in st:
+                used += int(s_.guess_used)
+                ratios.append(s_.guess_norm / s_.plain_norm if s_.plain_norm > 0 else 1.0)
+        torch.cuda.synchronize()
+        wall_l = time.perf_counter() - T0
+        sol_l = [h.get_solution() for h in bl.handles]
+        for q in nets:
+            q.close()
+        bl.close()
+        dvl = []
+        for a, c in zip(sol_l, sol_b):
+            a3, c3 = a.reshape(-1, 3), c.reshape(-1, 3)
+            dvl.append(float(np.linalg.norm(a3[:, :2] - c3[:, :2]) / max(np.linalg.norm(c3[:, :2]), 1e-300)))
+        learned = {"value": n * steps / wall_l, "unit": "instance-steps/s", "speedup_vs_one_by_one": wall_seq / wall_l,
+                   "latency_ms": {"p50": float(np.percentile(lat_l, 50)), "p99": float(np.percentile(lat_l, 99))},
+                   "gmres_iters": int(its_l), "guess_used": f"{used}/{n * steps}",
+                   "guess_residual_ratio_mean": float(np.mean(ratios)),
+                   "training": {"samples": int(nsamples), "iters": args.train_iters, "seconds": t_train,
+                                "loss_first_last": [float(losses[0]), float(losses[-1])],
+                                "samples_from": f"steps 2..{warm - 1} of every instance"},
+                   "max_velocity_rel_diff_vs_constant_predictor": max(dvl)}
+
     # the same batch in mixed precision (FP64 flexible GMRES around FP32 BiCGStab,
     # FP64 refinement and Newton residual), same steps and schedule rule
     mixed = None
@@ -1027,6 +1085,7 @@ def run_batch(args, world, rank, local):
                                  "batch_step_over_bound": float(wall_b * 1e3 / steps / lat_mat.max(axis=1).mean())},
             "instances_bitwise_equal_to_one_by_one": f"{equal}/{n}", "gpu_launches": int(launches),
             "extrapolation_guess_batch": extrap,
+            "shared_learned_guess_batch": learned,
             "mixed_precision_batch": mixed,
             "clocks": ck}
     return line

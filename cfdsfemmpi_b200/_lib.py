@@ -24,6 +24,7 @@ EXPORTS = [
     "cfdgpu_ilu_export", "cfdgpu_pc_apply_export",
     "cfdgpu_mpnn_create", "cfdgpu_mpnn_destroy", "cfdgpu_mpnn_num_params", "cfdgpu_mpnn_get_params",
     "cfdgpu_mpnn_set_params", "cfdgpu_mpnn_set_scales", "cfdgpu_mpnn_add_sample", "cfdgpu_mpnn_num_samples",
+    "cfdgpu_mpnn_set_condition", "cfdgpu_mpnn_add_sample_on",
     "cfdgpu_mpnn_loss_grad", "cfdgpu_mpnn_train", "cfdgpu_mpnn_predict", "cfdgpu_set_guess_mode", "cfdgpu_set_guess",
     "cfdgpu_batch_create", "cfdgpu_batch_destroy", "cfdgpu_batch_last_error", "cfdgpu_batch_size",
     "cfdgpu_batch_handle", "cfdgpu_batch_set_schedule", "cfdgpu_batch_get_schedule", "cfdgpu_batch_step",
@@ -130,6 +131,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_mpnn_set_params.argtypes = [vp, vp]
     L.cfdgpu_mpnn_set_scales.argtypes = [vp, vp, vp]
     L.cfdgpu_mpnn_add_sample.argtypes = [vp, vp, vp, vp]
+    L.cfdgpu_mpnn_set_condition.argtypes = [vp, dp]
+    L.cfdgpu_mpnn_add_sample_on.argtypes = [vp, vp, dp, vp, vp, vp]
     L.cfdgpu_mpnn_num_samples.argtypes = [vp]
     L.cfdgpu_mpnn_loss_grad.argtypes = [vp, ip, vp, vp]
     L.cfdgpu_mpnn_train.argtypes = [vp, ip, ctypes.c_float, vp]
@@ -485,9 +488,22 @@ class Mpnn:
         b = np.ascontiguousarray(out_scale, dtype=np.float32)
         self._check(self._L.cfdgpu_mpnn_set_scales(self.m, _ptr(a), _ptr(b)))
 
-    def add_sample(self, u_nm1, u_n, u_np1):
+    def add_sample(self, u_nm1, u_n, u_np1, handle=None, cond=None):
+        """A training sample (u_{n-1}, u_n -> u_{n+1}) on the network's own
+        mesh, or on `handle`'s mesh (at most as many nodes) with condition
+        value `cond`."""
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u_nm1, u_n, u_np1)]
-        self._check(self._L.cfdgpu_mpnn_add_sample(self.m, *[_ptr(a) for a in arrs]))
+        if handle is None:
+            if cond is not None:
+                self.set_condition(cond)
+            self._check(self._L.cfdgpu_mpnn_add_sample(self.m, *[_ptr(a) for a in arrs]))
+        else:
+            self._check(self._L.cfdgpu_mpnn_add_sample_on(self.m, handle.h, float(cond or 0.0),
+                                                          *[_ptr(a) for a in arrs]))
+
+    def set_condition(self, cond: float):
+        """Condition input channel for the own graph's samples and predictions."""
+        self._check(self._L.cfdgpu_mpnn_set_condition(self.m, float(cond)))
 
     @property
     def num_samples(self) -> int:

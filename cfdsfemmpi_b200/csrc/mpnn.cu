@@ -85,6 +85,19 @@ struct cfdgpu_mpnn {
   std::vector<bf16 *> sx;
   std::vector<float *> st;
   float *mask = nullptr;             // N x FOUT, 1 on free dofs
+  // the mesh graphs samples live on: [0] the graph of the handle the network
+  // was created on (the one its predictions serve), then graphs of other
+  // handles whose samples train the same weights (at most as many nodes);
+  // g, N, mask, xlo, xinv above hold the graph in use
+  struct Graph {
+    cfdgpu::GraphView g;
+    int N;
+    float *mask;
+    double3 xlo, xinv;
+  };
+  std::vector<Graph> graphs;
+  std::vector<int> sg;               // graph of each sample
+  float cond = 0.f;                  // condition input channel (e.g. a scaled Reynolds number)
   std::vector<void *> allocs;
   std::string err;
 };
@@ -221,7 +234,8 @@ __global__ void k_mean_agg(int N, const int32_t *__restrict__ rowptr, const int3
 // input features of one sample / prediction
 __global__ void k_features(int N, int ndof, int ndim, const double *__restrict__ un, const double *__restrict__ unm1,
                            const double *__restrict__ coords, float s0, float s1, float s2, float s3, float d0,
-                           float d1, float d2, float d3, double3 xlo, double3 xinv, bf16 *__restrict__ X)
+                           float d1, float d2, float d3, double3 xlo, double3 xinv, float cond,
+                           bf16 *__restrict__ X)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -237,6 +251,8 @@ __global__ void k_features(int N, int ndof, int ndim, const double *__restrict__
   // coordinates mapped from the mesh's bounding box to [-1, 1] (2X - 1 on the unit square / cube)
   const double lo[3] = {xlo.x, xlo.y, xlo.z}, inv[3] = {xinv.x, xinv.y, xinv.z};
   for (int c = 0; c < ndim; c++) f[2 * ndof + c] = (float)(2.0 * ((coords[(int64_t)i * ndim + c] - lo[c]) * inv[c]) - 1.0);
+  // the condition channel (0 unless set)
+  f[2 * ndof + ndim] = cond;
 #pragma unroll
   for (int c = 0; c < FIN; c++) X[(int64_t)i * FIN + c] = __float2bfloat16(f[c]);
 }
@@ -511,13 +527,46 @@ int backward(cfdgpu_mpnn *m, const bf16 *X, const float *T, float *loss_dev)
   return cudaGetLastError() == cudaSuccess ? 0 : CFDGPU_ECUDA;
 }
 
+// make graph k the one the kernels use (the creator's stream always)
+void use_graph(cfdgpu_mpnn *m, int k)
+{
+  const cudaStream_t s = m->graphs[0].g.stream;
+  const cfdgpu_mpnn::Graph &G = m->graphs[k];
+  m->g = G.g;
+  m->g.stream = s;
+  m->N = G.N;
+  m->mask = G.mask;
+  m->xlo = G.xlo;
+  m->xinv = G.xinv;
+}
+
+// bounding box of a graph's nodes (lower corner, 1 / extent per axis)
+int graph_box(const cfdgpu::GraphView &g, double3 &xlo, double3 &xinv)
+{
+  std::vector<double> X((size_t)g.nNode * g.ndim);
+  if (cudaMemcpy(X.data(), g.coords, sizeof(double) * X.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CFDGPU_ECUDA;
+  double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  for (int c = 0; c < g.ndim; c++) {
+    lo[c] = hi[c] = X[c];
+    for (int i = 0; i < g.nNode; i++) {
+      lo[c] = std::min(lo[c], X[(size_t)i * g.ndim + c]);
+      hi[c] = std::max(hi[c], X[(size_t)i * g.ndim + c]);
+    }
+    if (!(hi[c] > lo[c])) hi[c] = lo[c] + 1.0;
+  }
+  xlo = make_double3(lo[0], lo[1], lo[2]);
+  xinv = make_double3(1.0 / (hi[0] - lo[0]), 1.0 / (hi[1] - lo[1]), 1.0 / (hi[2] - lo[2]));
+  return 0;
+}
+
 int sample_features(cfdgpu_mpnn *m, const double *d_unm1, const double *d_un, bf16 *X)
 {
   const int N = m->N;
   k_features<<<(N + 255) / 256, 256, 0, m->g.stream>>>(N, m->g.ndof, m->g.ndim, d_un, d_unm1, m->g.coords,
                                                        m->in_scale[0], m->in_scale[1], m->in_scale[2],
                                                        m->in_scale[3], m->in_scale[4], m->in_scale[5],
-                                                       m->in_scale[6], m->in_scale[7], m->xlo, m->xinv, X);
+                                                       m->in_scale[6], m->in_scale[7], m->xlo, m->xinv, m->cond, X);
   return cudaGetLastError() == cudaSuccess ? 0 : CFDGPU_ECUDA;
 }
 
@@ -581,23 +630,9 @@ int cfdgpu_mpnn_create(cfdgpu_handle *h, uint64_t seed, cfdgpu_mpnn **out)
     for (int i = 0; i < K * NO; i++) p[weight_off(m->L, w) + i] = a * uni(gen);
   }
   cudaMemcpy(m->P, p.data(), sizeof(float) * p.size(), cudaMemcpyHostToDevice);
-  {
-    std::vector<double> X((size_t)m->N * m->g.ndim);
-    if (cudaMemcpy(X.data(), m->g.coords, sizeof(double) * X.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
-      m->err = "coordinate copy failed";
-      return CFDGPU_ECUDA;
-    }
-    double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
-    for (int c = 0; c < m->g.ndim; c++) {
-      lo[c] = hi[c] = X[c];
-      for (int i = 0; i < m->N; i++) {
-        lo[c] = std::min(lo[c], X[(size_t)i * m->g.ndim + c]);
-        hi[c] = std::max(hi[c], X[(size_t)i * m->g.ndim + c]);
-      }
-      if (!(hi[c] > lo[c])) hi[c] = lo[c] + 1.0;
-    }
-    m->xlo = make_double3(lo[0], lo[1], lo[2]);
-    m->xinv = make_double3(1.0 / (hi[0] - lo[0]), 1.0 / (hi[1] - lo[1]), 1.0 / (hi[2] - lo[2]));
+  if ((rc = graph_box(m->g, m->xlo, m->xinv))) {
+    m->err = "coordinate copy failed";
+    return rc;
   }
   // activations
   if ((rc = dalloc(m, &m->X, (size_t)Np * FIN)) || (rc = dalloc(m, &m->Ze, (size_t)Np * HID)) ||
@@ -617,6 +652,7 @@ int cfdgpu_mpnn_create(cfdgpu_handle *h, uint64_t seed, cfdgpu_mpnn **out)
   while (Np % m->nchunks) m->nchunks--;
   if ((rc = dalloc(m, &m->partial, (size_t)m->nchunks * (2 * HID + 1) * HID))) return rc;
   k_mask<<<(m->N + 255) / 256, 256, 0, m->g.stream>>>(m->N, m->g.ndof, m->g.fixmask, m->mask);
+  m->graphs.push_back({m->g, m->N, m->mask, m->xlo, m->xinv});
   if ((rc = refresh_bf16(m))) return rc;
   if (cudaStreamSynchronize(m->g.stream) != cudaSuccess) return CFDGPU_ECUDA;
   return 0;
@@ -685,7 +721,50 @@ int cfdgpu_mpnn_add_sample(cfdgpu_mpnn *m, const double *u_nm1, const double *u_
   if (rc || cudaGetLastError() != cudaSuccess) return CFDGPU_ECUDA;
   m->sx.push_back(X);
   m->st.push_back(T);
+  m->sg.push_back(0);
   return 0;
+}
+
+int cfdgpu_mpnn_set_condition(cfdgpu_mpnn *m, double cond)
+{
+  if (!m || !std::isfinite(cond)) return CFDGPU_EINVAL;
+  m->cond = (float)cond;
+  return 0;
+}
+
+int cfdgpu_mpnn_add_sample_on(cfdgpu_mpnn *m, cfdgpu_handle *h, double cond, const double *u_nm1, const double *u_n,
+                              const double *u_np1)
+{
+  if (!m || !h || !u_nm1 || !u_n || !u_np1 || !std::isfinite(cond)) return CFDGPU_EINVAL;
+  cfdgpu::GraphView gv;
+  int rc = cfdgpu::handle_graph(h, &gv);
+  if (rc) return rc;
+  const cfdgpu_mpnn::Graph &G0 = m->graphs[0];
+  if (gv.ndof != G0.g.ndof || gv.ndim != G0.g.ndim || gv.nNode > G0.N) {
+    m->err = "sample graph: other dof count, dimension, or more nodes than the network's own graph";
+    return CFDGPU_EINVAL;
+  }
+  int k = -1;
+  for (size_t q = 0; q < m->graphs.size(); q++)
+    if (m->graphs[q].g.rowptr == gv.rowptr) k = (int)q;
+  if (k < 0) {
+    cfdgpu_mpnn::Graph G{gv, gv.nNode, nullptr, {}, {}};
+    if ((rc = graph_box(gv, G.xlo, G.xinv))) return rc;
+    if ((rc = dalloc(m, &G.mask, (size_t)m->Npad * FOUT))) return rc;
+    k_mask<<<(G.N + 255) / 256, 256, 0, G0.g.stream>>>(G.N, gv.ndof, gv.fixmask, G.mask);
+    m->graphs.push_back(G);
+    k = (int)m->graphs.size() - 1;
+  }
+  // the other handle's stream may still be writing what it returns: finish it
+  if (cudaStreamSynchronize(gv.stream) != cudaSuccess) return CFDGPU_ECUDA;
+  const float keep = m->cond;
+  use_graph(m, k);
+  m->cond = (float)cond;
+  rc = cfdgpu_mpnn_add_sample(m, u_nm1, u_n, u_np1);
+  m->cond = keep;
+  if (!rc) m->sg.back() = k;
+  use_graph(m, 0);
+  return rc;
 }
 
 int cfdgpu_mpnn_num_samples(cfdgpu_mpnn *m) { return m ? (int)m->sx.size() : CFDGPU_EINVAL; }
@@ -693,8 +772,10 @@ int cfdgpu_mpnn_num_samples(cfdgpu_mpnn *m) { return m ? (int)m->sx.size() : CFD
 int cfdgpu_mpnn_loss_grad(cfdgpu_mpnn *m, int sample, float *loss, float *grad)
 {
   if (!m || sample < 0 || sample >= (int)m->sx.size()) return CFDGPU_EINVAL;
+  use_graph(m, m->sg[sample]);
   int rc = forward(m, m->sx[sample]);
   if (!rc) rc = backward(m, m->sx[sample], m->st[sample], m->lossbuf);
+  use_graph(m, 0);
   if (rc) return rc;
   if (loss) cudaMemcpyAsync(loss, m->lossbuf, sizeof(float), cudaMemcpyDeviceToHost, m->g.stream);
   if (grad) cudaMemcpyAsync(grad, m->G, sizeof(float) * m->L.total, cudaMemcpyDeviceToHost, m->g.stream);
@@ -708,14 +789,19 @@ int cfdgpu_mpnn_train(cfdgpu_mpnn *m, int iters, float lr, float *loss_out)
   const int S = (int)m->sx.size();
   for (int it = 0; it < iters; it++) {
     const int smp = (int)(m->step % S);
+    use_graph(m, m->sg[smp]);
     int rc = forward(m, m->sx[smp]);
     if (!rc) rc = backward(m, m->sx[smp], m->st[smp], m->lossbuf);
-    if (rc) return rc;
+    if (rc) {
+      use_graph(m, 0);
+      return rc;
+    }
     m->step++;
     const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
     k_adam<<<(m->L.total + 255) / 256, 256, 0, m->g.stream>>>(m->L.total, m->P, m->G, m->Am, m->Av, lr, b1, b2, eps, c1, c2);
     if ((rc = refresh_bf16(m))) return rc;
   }
+  use_graph(m, 0);
   if (loss_out) cudaMemcpyAsync(loss_out, m->lossbuf, sizeof(float), cudaMemcpyDeviceToHost, m->g.stream);
   return cudaStreamSynchronize(m->g.stream) == cudaSuccess ? 0 : CFDGPU_ECUDA;
 }

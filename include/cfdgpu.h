@@ -295,6 +295,18 @@ int cfdgpu_mpnn_set_params(cfdgpu_mpnn *m, const float *p);
 int cfdgpu_mpnn_set_scales(cfdgpu_mpnn *m, const float *in_scale, const float *out_scale);
 /* one training sample (host arrays of nNode*ndof): u_{n-1}, u_n, u_{n+1} */
 int cfdgpu_mpnn_add_sample(cfdgpu_mpnn *m, const double *u_nm1, const double *u_n, const double *u_np1);
+/* Condition input channel (a per-instance scalar such as a scaled Reynolds
+ * number; 0 by default): used by later samples of the network's own graph
+ * and by its predictions. */
+int cfdgpu_mpnn_set_condition(cfdgpu_mpnn *m, double cond);
+/* A training sample (host arrays) on another handle's mesh graph, with its
+ * condition value: one network's weights learn from instances of different
+ * meshes.  The other mesh must have the same dofs per node and dimension and
+ * at most as many nodes as the network's own; predictions always serve the
+ * network's own handle (copy trained weights into a network per instance
+ * with cfdgpu_mpnn_get_params / cfdgpu_mpnn_set_params). */
+int cfdgpu_mpnn_add_sample_on(cfdgpu_mpnn *m, cfdgpu_handle *h, double cond, const double *u_nm1, const double *u_n,
+                              const double *u_np1);
 int cfdgpu_mpnn_num_samples(cfdgpu_mpnn *m);
 /* masked mean-squared error of one sample and its gradient (host floats) */
 int cfdgpu_mpnn_loss_grad(cfdgpu_mpnn *m, int sample, float *loss, float *grad);

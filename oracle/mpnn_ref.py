@@ -46,7 +46,7 @@ def unpack(p):
     return out
 
 
-def features(u_nm1, u_n, coords, ndof, ndim, in_scale):
+def features(u_nm1, u_n, coords, ndof, ndim, in_scale, cond=0.0):
     N = coords.shape[0]
     f = np.zeros((N, FIN), np.float32)
     un = u_n.reshape(N, ndof)
@@ -58,6 +58,7 @@ def features(u_nm1, u_n, coords, ndof, ndim, in_scale):
         lo, hi = coords[:, c].min(), coords[:, c].max()
         inv = 1.0 / (hi - lo) if hi > lo else 1.0
         f[:, 2 * ndof + c] = (2.0 * ((coords[:, c] - lo) * inv) - 1.0).astype(np.float32)
+    f[:, 2 * ndof + ndim] = np.float32(cond)
     return bf16(f)
 
 

@@ -223,3 +223,101 @@ def test_guess_directions_cover_systems_above_one_grid_of_threads():
     assert all(s["converged"] for s in stats)
     for s in stats[2:]:
         assert s["guess_used"] and s["guess_norm"] < 0.5 * s["plain_norm"], s
+
+
+def _mesh_sample_ref(h, mesh, u, in_s, out_s, cond, p):
+    d = h.export_pattern()
+    X = mpnn_ref.features(u[0], u[1], mesh.coords, 3, 2, in_s, cond)
+    T = mpnn_ref.targets(u[0], u[1], u[2], 3, out_s)
+    mask = np.zeros((mesh.nNode, mpnn_ref.FOUT), np.float32)
+    free = (d["dofmap"].reshape(-1, 3) >= 0)
+    mask[:, :3] = free
+    return mpnn_ref.loss_and_grad(p, X, T, mask, d["rowptr"], d["colidx"], int(free.sum()))
+
+
+def test_shared_network_samples_on_other_meshes_and_conditions():
+    """One network trained on instances of different meshes and Reynolds
+    numbers (the batched sweep's shared, Re-conditioned guess): a sample on
+    another handle's smaller mesh, with its own condition value, gives the
+    loss and gradients of the CPU reference on that mesh (the network's
+    padding rows contribute nothing), as does a sample on its own mesh with
+    a condition."""
+    meshes = [meshgen.cavity2d(10), meshgen.cavity2d(7)]
+    ctrl = meshgen.control_for(3, 0.05, 0.01)
+    hs = [Handle(m, ctrl) for m in meshes]
+    net = Mpnn(hs[0], seed=5)
+    rng = np.random.default_rng(3)
+    in_s = np.array([0.1, 0.1, 0.05, 0.02, 0.02, 0.01], np.float32)   # u (u, v, p), then u_n - u_{n-1}
+    out_s = np.array([0.02, 0.02, 0.01], np.float32)
+    net.set_scales(in_s, out_s)
+    conds = [0.6, 0.9]
+    us = [[0.1 * rng.standard_normal(h.n) for _ in range(3)] for h in hs]
+    net.add_sample(*us[0], cond=conds[0])
+    net.add_sample(*us[1], handle=hs[1], cond=conds[1])
+    p = net.get_params()
+    off, _ = _blocks()
+    o = off["Wd"]
+    p[o[0]:o[0] + o[1] * o[2]] = 0.2 * rng.standard_normal(o[1] * o[2]).astype(np.float32)
+    net.set_params(p)
+    for k in range(2):
+        loss_gpu, g_gpu = net.loss_grad(k)
+        loss_ref, g_ref = _mesh_sample_ref(hs[k], meshes[k], us[k], in_s, out_s, conds[k], p)
+        assert abs(loss_gpu - loss_ref) <= 1e-4 * abs(loss_ref), (k, loss_gpu, loss_ref)
+        for name, ob in off.items():
+            size = ob[1] * ob[2] if len(ob) == 3 else ob[1]
+            a = g_gpu[ob[0]:ob[0] + size]
+            b = g_ref[ob[0]:ob[0] + size]
+            if np.abs(b).max() == 0:
+                assert np.abs(a).max() == 0, (k, name)
+                continue
+            assert np.abs(a - b).max() / np.abs(b).max() < 2e-2, (k, name)
+    # a mesh with more nodes than the network's own is refused
+    big = Handle(meshgen.cavity2d(12), ctrl)
+    with pytest.raises(Exception):
+        net.add_sample(*[np.zeros(big.n)] * 3, handle=big, cond=0.5)
+    big.close()
+    net.close()
+    for h in hs:
+        h.close()
+
+
+def test_shared_network_guides_every_instance_of_a_batch():
+    """The shared, Re-conditioned network trained on the first steps of a
+    batch of cavities of different sizes and Reynolds numbers is attached to
+    every instance (its own condition value): every later step converges,
+    and the answers stay those of the batch without it (velocity to 1e-6;
+    every solve stops at rtol 1e-8 relative to its own start)."""
+    from cfdsfemmpi_b200 import Batch
+    from cfdsfemmpi_b200.surrogate import attach_shared, train_shared
+    cases = meshgen.batch_cases(count=3, n_lo=8, n_hi=14, dt=0.05, steps=20, seed=7)
+    pairs = [(m, c) for m, c, _, _ in cases]
+    conds = [float(np.log(re) / np.log(5000.0)) for _, _, _, re in cases]
+    kw = dict(restart=200, rtol=1e-8, pc="pbjacobi", max_it=20000)
+    out = []
+    for learned in (False, True):
+        b = Batch(pairs, **kw)
+        b.set_schedule(3, 4, 1)
+        trajs = [[h.get_solution()] for h in b.handles]
+        for k in range(12):
+            b.step(np.full(len(pairs), 0.05 * (k + 1)))
+            for i, h in enumerate(b.handles):
+                trajs[i].append(h.get_solution())
+        nets = []
+        if learned:
+            net0, shared, losses = train_shared(b.handles, trajs, conds, iters=600, lr=2e-3, seed=0, first=2)
+            assert net0.num_samples == 3 * 10 and losses[-1] < losses[0]
+            net0.close()
+            nets = [attach_shared(h, shared, c) for h, c in zip(b.handles, conds)]
+        stats = []
+        for k in range(12, 16):
+            st, _ = b.step(np.full(len(pairs), 0.05 * (k + 1)))
+            stats.extend(s.as_dict() for s in st)
+        out.append(([h.get_solution().reshape(-1, 3) for h in b.handles], stats))
+        for q in nets:
+            q.close()
+        b.close()
+    (base, _), (guided, st) = out
+    assert all(s["converged"] for s in st)
+    assert any(s["guess_used"] for s in st)
+    for a, c in zip(guided, base):
+        assert np.linalg.norm(a[:, :2] - c[:, :2]) / np.linalg.norm(c[:, :2]) < 1e-6
