@@ -107,6 +107,8 @@ def parse():
                    help="kernels: GMRES restart of the bounded profiling case")
     p.add_argument("--kernel-its", type=int, default=40,
                    help="kernels: GMRES iterations of the bounded profiling case")
+    p.add_argument("--kernel-net", action="store_true",
+                   help="kernels: also one forward pass of the guess network (random weights) on the workload's mesh")
     p.add_argument("--no-batch-mixed", action="store_true", help="batch: skip the mixed-precision batch arm")
     p.add_argument("--no-batch-learned", action="store_true",
                    help="batch: skip the arm with the shared, Re-conditioned guess network")
@@ -1118,10 +1120,15 @@ def run_kernels(args, local):
     b = rng.standard_normal(n)
     b[h.export_pattern()["fixed_dofs"]] = 0.0
     x, its, reason = h.solve_export(b)
+    if args.kernel_net:
+        from cfdsfemmpi_b200._lib import Mpnn
+        net = Mpnn(h, seed=0)
+        net.predict(prev, 0.5 * prev)
+        net.close()
     dt = time.perf_counter() - t0
     line = {"method": "kernels", "workload": args.workload, "nodes": mesh.nNode, "solver": solver_label(kw),
             "restart": args.kernel_restart, "its": its, "reason": reason, "seconds": dt,
-            "launches": h.launch_count()}
+            "launches": h.launch_count(), "network_forward": bool(args.kernel_net)}
     h.close()
     return line
 
