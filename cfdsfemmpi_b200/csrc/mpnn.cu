@@ -127,21 +127,29 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
 // C[Npad x NO] = A[Npad x K] (bf16, row-major) * W (bf16, given as Wt = NO x K
 // row-major, i.e. the "col" operand of mma.sync) + bias (optional), FP32
 // accumulation and FP32 output.  One warp computes 16 rows x NO columns
-// (NO/8 m16n8k16 tiles per k-step of 16); 4 warps per CTA; the weights are
-// staged in shared memory once per CTA.
+// (NO/8 m16n8k16 tiles per k-step of 16); 4 warps per CTA, each CTA walking
+// 64-row tiles with a grid stride.  The weights are staged in shared memory
+// once per CTA with rows padded to K + 8 elements, so the eight row groups of
+// a fragment read fall in distinct banks (unpadded, a 256-byte row stride put
+// them all in one bank: an 8-way conflict that made the kernel bound by
+// shared-memory bandwidth).
 template <int K, int NO>
 __global__ void __launch_bounds__(128)
 gemm_bf16(int Npad, const bf16 *__restrict__ A, const bf16 *__restrict__ Wt, const float *__restrict__ bias,
           float *__restrict__ C)
 {
-  __shared__ __align__(16) bf16 sW[NO * K];
-  for (int i = threadIdx.x; i < NO * K / 2; i += blockDim.x)
-    reinterpret_cast<uint32_t *>(sW)[i] = reinterpret_cast<const uint32_t *>(Wt)[i];
+  constexpr int KP = K + 8;
+  __shared__ __align__(16) bf16 sW[NO * KP];
+  for (int i = threadIdx.x; i < NO * K / 2; i += blockDim.x) {
+    const int rr = (2 * i) / K, cc = (2 * i) % K;
+    *reinterpret_cast<uint32_t *>(sW + rr * KP + cc) = reinterpret_cast<const uint32_t *>(Wt)[i];
+  }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r0 = blockIdx.x * ROWS_PER_CTA + warp * 16;
-  if (r0 >= Npad) return;
   const int gq = lane >> 2, tq = lane & 3;
+  const int ntiles = Npad / ROWS_PER_CTA;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  const int r0 = tile * ROWS_PER_CTA + warp * 16;
   float acc[NO / 8][4];
 #pragma unroll
   for (int t = 0; t < NO / 8; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
@@ -156,7 +164,7 @@ gemm_bf16(int Npad, const bf16 *__restrict__ A, const bf16 *__restrict__ Wt, con
     a[3] = *reinterpret_cast<const uint32_t *>(ar1 + 8);
 #pragma unroll
     for (int t = 0; t < NO / 8; t++) {
-      const bf16 *bp = sW + (t * 8 + gq) * K + k0 + 2 * tq;
+      const bf16 *bp = sW + (t * 8 + gq) * KP + k0 + 2 * tq;
       const uint32_t b0 = *reinterpret_cast<const uint32_t *>(bp);
       const uint32_t b1 = *reinterpret_cast<const uint32_t *>(bp + 8);
       mma_bf16(acc[t], a, b0, b1);
@@ -171,7 +179,11 @@ gemm_bf16(int Npad, const bf16 *__restrict__ A, const bf16 *__restrict__ Wt, con
     *reinterpret_cast<float2 *>(C + (int64_t)(r0 + gq) * NO + c) = v0;
     *reinterpret_cast<float2 *>(C + (int64_t)(r0 + gq + 8) * NO + c) = v1;
   }
+  }
 }
+
+// CTAs of gemm_bf16 for Npad rows: one per 64-row tile, at most 8 per SM
+inline int gemm_grid(int Npad) { return std::max(1, std::min(Npad / ROWS_PER_CTA, 148 * 8)); }
 
 // h = relu(z) (encoder) or h = hprev + relu(z) (residual layers); writes the
 // FP32 result and its BF16 copy into column block [0, HID) of the next
@@ -464,7 +476,7 @@ int forward(cfdgpu_mpnn *m, const bf16 *X)
 {
   cudaStream_t s = m->g.stream;
   const int Np = m->Npad;
-  const int gridg = Np / ROWS_PER_CTA;
+  const int gridg = gemm_grid(Np);
   const PLayout &L = m->L;
   const int64_t cnt = (int64_t)Np * HID;
   gemm_bf16<FIN, HID><<<gridg, 128, 0, s>>>(Np, X, m->Wb + m->wb_off[1], m->P + L.be, m->Ze);
@@ -502,7 +514,7 @@ int backward(cfdgpu_mpnn *m, const bf16 *X, const float *T, float *loss_dev)
 {
   cudaStream_t s = m->g.stream;
   const int Np = m->Npad;
-  const int gridg = Np / ROWS_PER_CTA;
+  const int gridg = gemm_grid(Np);
   const int64_t cnt = (int64_t)Np * HID;
   const int64_t ycnt = (int64_t)Np * FOUT;
   const float inv_cnt = 1.f / (float)std::max(1, m->g.nfree);
