@@ -74,8 +74,15 @@ def test_ldc3d_32_matches_oracle_with_bench_options(steps):
         with open(path, "a") as f:
             f.write(json.dumps(rec) + "\n")
     assert err <= max(1e-8, 2.0 * spread), rec
-    # same Newton structure; BiCGStab counts within max(3, 10 %) on every
-    # solve: the count moves with summation order alone (the oracle's own
-    # runs gave 81, 83, 85 and 91 iterations on step 10)
-    assert [len(a) for a in its_gpu] == [len(b) for b in its_all]
-    assert all(abs(x - y) <= max(3, 0.1 * y) for a, b in zip(its_gpu, its_all) for x, y in zip(a, b)), rec
+    # same Newton structure; BiCGStab counts within max(3, 10 %, 2 x the
+    # oracle's own one-thread/all-thread difference) on every solve, and
+    # within 3 % on average: the count moves with summation order alone (the
+    # oracle's own runs gave 81, 83, 85 and 91 iterations on step 10, 94 and
+    # 101 on step 20)
+    assert [len(a) for a in its_gpu] == [len(b) for b in its_all] == [len(c) for c in its_one]
+    for a, b, c in zip(its_gpu, its_all, its_one):
+        for x, y, y1 in zip(a, b, c):
+            assert abs(x - y) <= max(3, 0.1 * y, 2 * abs(y1 - y)), rec
+    tot_gpu = sum(sum(a) for a in its_gpu)
+    tot_all = sum(sum(b) for b in its_all)
+    assert abs(tot_gpu - tot_all) <= 0.03 * tot_all, rec
