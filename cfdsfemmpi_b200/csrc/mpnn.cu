@@ -132,14 +132,20 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
 // once per CTA with rows padded to K + 8 elements, so the eight row groups of
 // a fragment read fall in distinct banks (unpadded, a 256-byte row stride put
 // them all in one bank: an 8-way conflict that made the kernel bound by
-// shared-memory bandwidth).
+// shared-memory bandwidth).  Each warp copies its 16 rows of A into shared
+// memory with 16-byte asynchronous copies (padded the same way) and reads its
+// fragments from there: fragment loads straight from global memory touch
+// eight rows per instruction and bound the kernel at L1.
 template <int K, int NO>
 __global__ void __launch_bounds__(128)
 gemm_bf16(int Npad, const bf16 *__restrict__ A, const bf16 *__restrict__ Wt, const float *__restrict__ bias,
           float *__restrict__ C)
 {
   constexpr int KP = K + 8;
+  constexpr int CPR = K / 8;                    // 16-byte chunks per row of A
+  static_assert(K % 8 == 0, "rows of A in 16-byte chunks");
   __shared__ __align__(16) bf16 sW[NO * KP];
+  __shared__ __align__(16) bf16 sA[4][16 * KP];
   for (int i = threadIdx.x; i < NO * K / 2; i += blockDim.x) {
     const int rr = (2 * i) / K, cc = (2 * i) % K;
     *reinterpret_cast<uint32_t *>(sW + rr * KP + cc) = reinterpret_cast<const uint32_t *>(Wt)[i];
@@ -150,14 +156,23 @@ gemm_bf16(int Npad, const bf16 *__restrict__ A, const bf16 *__restrict__ Wt, con
   const int ntiles = Npad / ROWS_PER_CTA;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
   const int r0 = tile * ROWS_PER_CTA + warp * 16;
+  bf16 *const wa = sA[warp];
+  for (int q = lane; q < 16 * CPR; q += 32) {
+    const int rr = q / CPR, cc = (q % CPR) * 8;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(wa + rr * KP + cc)),
+                 "l"(A + (int64_t)(r0 + rr) * K + cc)
+                 : "memory");
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncwarp();
   float acc[NO / 8][4];
 #pragma unroll
   for (int t = 0; t < NO / 8; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
 #pragma unroll
   for (int k0 = 0; k0 < K; k0 += 16) {
     uint32_t a[4];
-    const bf16 *ar0 = A + (int64_t)(r0 + gq) * K + k0 + 2 * tq;
-    const bf16 *ar1 = A + (int64_t)(r0 + gq + 8) * K + k0 + 2 * tq;
+    const bf16 *ar0 = wa + gq * KP + k0 + 2 * tq;
+    const bf16 *ar1 = wa + (gq + 8) * KP + k0 + 2 * tq;
     a[0] = *reinterpret_cast<const uint32_t *>(ar0);
     a[1] = *reinterpret_cast<const uint32_t *>(ar1);
     a[2] = *reinterpret_cast<const uint32_t *>(ar0 + 8);
@@ -179,6 +194,8 @@ gemm_bf16(int Npad, const bf16 *__restrict__ A, const bf16 *__restrict__ Wt, con
     *reinterpret_cast<float2 *>(C + (int64_t)(r0 + gq) * NO + c) = v0;
     *reinterpret_cast<float2 *>(C + (int64_t)(r0 + gq + 8) * NO + c) = v1;
   }
+  // every lane has read its fragments before the next tile's copy lands
+  __syncwarp();
   }
 }
 
