@@ -7,8 +7,9 @@ input/petsc_options_gmres.dat (GMRES(20)), both with block Jacobi and ILU(3)
 sub-solves.  The reference ships no solution for this case, so the GPU run is
 compared with the oracle running the same solver from rest on one host thread
 (OpenMP reductions combine in no fixed order, and BiCGStab's first solve from
-rest is chaotic: four oracle runs on eight threads took 306, 325 and 442
-iterations, the last ending in a breakdown, one thread 503).  Fields after the
+rest is chaotic: oracle runs on eight threads took 283 to 325 iterations or
+broke down when (r, r0) summed to exactly zero at rounding level, one thread
+503).  Fields after the
 first steps agree to max(1e-8, 2 x the distance between the oracle's
 BiCGStab and GMRES answers), which measures how far rtol 1e-10 determines the
 solution.  GMRES counts agree within max(3, 5 %) on every solve; BiCGStab's
