@@ -19,7 +19,7 @@ EXPORTS = [
     "cfdgpu_create", "cfdgpu_destroy", "cfdgpu_last_error", "cfdgpu_step", "cfdgpu_get_solution",
     "cfdgpu_set_solution", "cfdgpu_device_solution", "cfdgpu_stream", "cfdgpu_set_history", "cfdgpu_get_history",
     "cfdgpu_element_matrices", "cfdgpu_set_element_state", "cfdgpu_pattern_info_get", "cfdgpu_export_pattern",
-    "cfdgpu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
+    "cfdgpu_pattern_build", "cfdgpu_ilu_pattern_build", "cfdgpu_assemble_export", "cfdgpu_solve_export", "cfdgpu_timers", "cfdgpu_launch_count",
     "cfdgpu_set_profiling", "cfdgpu_kernel_stats", "cfdgpu_true_residual", "cfdgpu_residual_norm_noalloc",
     "cfdgpu_ilu_export", "cfdgpu_pc_apply_export",
     "cfdgpu_mpnn_create", "cfdgpu_mpnn_destroy", "cfdgpu_mpnn_num_params", "cfdgpu_mpnn_get_params",
@@ -85,6 +85,12 @@ class PatternInfo(ctypes.Structure):
                 ("nnzb", ctypes.c_int64), ("ncolors", ctypes.c_int), ("nfixed", ctypes.c_int), ("nfree", ctypes.c_int)]
 
 
+class IluInfo(ctypes.Structure):
+    _fields_ = [("nNode", ctypes.c_int), ("nnzb", ctypes.c_int64), ("nchains_l", ctypes.c_int),
+                ("nchains_u", ctypes.c_int), ("nlev_l", ctypes.c_int), ("nlev_u", ctypes.c_int),
+                ("chain_levels_l", ctypes.c_int), ("chain_levels_u", ctypes.c_int)]
+
+
 _LIB: Optional[ctypes.CDLL] = None
 
 
@@ -117,6 +123,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.cfdgpu_pattern_info_get.argtypes = [vp, ctypes.POINTER(PatternInfo)]
     L.cfdgpu_export_pattern.argtypes = [vp] + [vp] * 8
     L.cfdgpu_pattern_build.argtypes = [ctypes.POINTER(Mesh), ctypes.POINTER(PatternInfo)] + [vp] * 8
+    L.cfdgpu_ilu_pattern_build.argtypes = [ctypes.POINTER(Mesh), ip, ip, ctypes.POINTER(IluInfo)] + [vp] * 9
     L.cfdgpu_assemble_export.argtypes = [vp, ip, vp, vp]
     L.cfdgpu_solve_export.argtypes = [vp, vp, vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.cfdgpu_timers.argtypes = [vp, vp]
@@ -216,6 +223,34 @@ def pattern_build(mesh) -> dict:
     d["colidx"] = d["colidx"][:pi.nnzb]
     d["fixed_dofs"] = d["fixed_dofs"][:pi.nfixed]
     d["info"] = pi
+    return d
+
+
+def ilu_pattern_build(mesh, levels: int = 0, nblocks: int = 1) -> dict:
+    """Host-only block ILU(k) symbolic phase and its schedules
+    (cfdgpu_ilu_pattern_build); needs no GPU."""
+    L = load()
+    m, keep = _mesh_struct(mesh)
+    info = IluInfo()
+    rc = L.cfdgpu_ilu_pattern_build(ctypes.byref(m), levels, nblocks, ctypes.byref(info), *([None] * 9))
+    if rc != 0:
+        raise CfdGpuError(rc, "ILU pattern build failed")
+    n = info.nNode
+    d = {"rowptr": np.zeros(n + 1, np.int32), "colidx": np.zeros(max(info.nnzb, 1), np.int32),
+         "perm": np.zeros(n, np.int32), "lorder": np.zeros(n, np.int32), "uorder": np.zeros(n, np.int32),
+         "lchain": np.zeros(2 * max(info.nchains_l, 1), np.int32), "uchain": np.zeros(2 * max(info.nchains_u, 1), np.int32),
+         "lchain_order": np.zeros(max(info.nchains_l, 1), np.int32),
+         "uchain_order": np.zeros(max(info.nchains_u, 1), np.int32)}
+    keys = ("rowptr", "colidx", "perm", "lorder", "uorder", "lchain", "uchain", "lchain_order", "uchain_order")
+    rc = L.cfdgpu_ilu_pattern_build(ctypes.byref(m), levels, nblocks, ctypes.byref(info), *[_ptr(d[k]) for k in keys])
+    if rc != 0:
+        raise CfdGpuError(rc, "ILU pattern build failed")
+    d["colidx"] = d["colidx"][:info.nnzb]
+    d["lchain"] = d["lchain"][:2 * info.nchains_l].reshape(-1, 2)
+    d["uchain"] = d["uchain"][:2 * info.nchains_u].reshape(-1, 2)
+    d["lchain_order"] = d["lchain_order"][:info.nchains_l]
+    d["uchain_order"] = d["uchain_order"][:info.nchains_u]
+    d["info"] = info
     return d
 
 

@@ -1704,6 +1704,38 @@ int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int
   return 0;
 }
 
+int cfdgpu_ilu_pattern_build(const cfdgpu_mesh *mesh, int levels, int nblocks, cfdgpu_ilu_info *info,
+                             int32_t *rowptr, int32_t *colidx, int32_t *perm, int32_t *lorder, int32_t *uorder,
+                             int32_t *lchain, int32_t *uchain, int32_t *lchain_order, int32_t *uchain_order)
+{
+  if (!mesh || !info || !mesh->conn) return CFDGPU_EINVAL;
+  Topology t;
+  std::string msg = build_topology(mesh->nNode, mesh->nElem, mesh->npElem, mesh->ndim + 1, mesh->conn, mesh->nDBC,
+                                   mesh->dbc_node, mesh->dbc_dof, mesh->dbc_value, t);
+  if (!msg.empty()) return CFDGPU_EINVAL;
+  IluPattern f;
+  msg = build_ilu_pattern(t, levels, nblocks, f);
+  if (!msg.empty()) return CFDGPU_EINVAL;
+  info->nNode = mesh->nNode;
+  info->nnzb = f.nnzb();
+  info->nchains_l = (int)f.lchain_order.size();
+  info->nchains_u = (int)f.uchain_order.size();
+  info->nlev_l = f.nlev_l;
+  info->nlev_u = f.nlev_u;
+  info->chain_levels_l = f.lchain_levels;
+  info->chain_levels_u = f.uchain_levels;
+  auto cp = [](int32_t *dst, const std::vector<int32_t> &v) { if (dst && !v.empty()) memcpy(dst, v.data(), v.size() * 4); };
+  cp(rowptr, f.rowptr); cp(colidx, f.colidx); cp(lorder, f.lorder); cp(uorder, f.uorder);
+  cp(lchain, f.lchain); cp(uchain, f.uchain); cp(lchain_order, f.lchain_order); cp(uchain_order, f.uchain_order);
+  if (perm) {
+    if (f.perm.empty())
+      for (int i = 0; i < mesh->nNode; i++) perm[i] = i;
+    else
+      cp(perm, f.perm);
+  }
+  return 0;
+}
+
 int cfdgpu_assemble_export(cfdgpu_handle *h, int iter, double *bsr_vals, double *rhs)
 {
   if (!h) return CFDGPU_EINVAL;

@@ -210,6 +210,29 @@ int cfdgpu_pattern_build(const cfdgpu_mesh *mesh, cfdgpu_pattern_info *info, int
                          int32_t *slot, int32_t *color, int32_t *color_ptr, int32_t *color_elems,
                          int32_t *fixed_dofs, int32_t *dofmap);
 
+/* Host-only: the block ILU(k) symbolic phase of the library (the factor
+ * pattern and the schedules of the persistent factorisation and triangular
+ * solves) for a mesh, levels (-1: complete factorisation) and block-Jacobi
+ * blocks.  Call once with NULL arrays to get the sizes, then with arrays of
+ * those sizes: rowptr (nNode+1), colidx (nnzb), perm (nNode; the identity
+ * unless the complete factorisation is reordered), lorder / uorder (nNode:
+ * rows in level order of the lower / upper dependency DAG), lchain / uchain
+ * (2 x nchains: first row, one past the last row), lchain_order /
+ * uchain_order (nchains: chain ids in chain-DAG level order).  Any pointer may
+ * be NULL.  Used by tests to check the schedules' invariants (every input of
+ * a row or chain is handed out earlier), on which the sync-free kernels'
+ * progress rests. */
+typedef struct cfdgpu_ilu_info {
+  int nNode;
+  int64_t nnzb;              /* factor blocks */
+  int nchains_l, nchains_u;
+  int nlev_l, nlev_u;        /* levels of the row DAGs */
+  int chain_levels_l, chain_levels_u;
+} cfdgpu_ilu_info;
+int cfdgpu_ilu_pattern_build(const cfdgpu_mesh *mesh, int levels, int nblocks, cfdgpu_ilu_info *info,
+                             int32_t *rowptr, int32_t *colidx, int32_t *perm, int32_t *lorder, int32_t *uorder,
+                             int32_t *lchain, int32_t *uchain, int32_t *lchain_order, int32_t *uchain_order);
+
 /* Assemble (iteration-0 semantics when iter == 0: lifting included) at the
  * current state and copy the BSR values (nnzb*ndof*ndof, FP64, block
  * row-major) and the RHS (nNode*ndof) to host.  Uses the td[] of the last
